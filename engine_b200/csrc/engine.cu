@@ -1,0 +1,1289 @@
+// Host side of the B200 parADMM engine: the C-ABI of paradmm_gpu.h and the
+// GPU-backed sweep functions of paradmm.h.
+//
+// Replaces the reference GPU back-end's host code (core/paradmm-gpu.cu:424-532
+// copyGraphFromCPUtoGPU and the launch loop of packing/gpu.cu:257-291).
+#include <dlfcn.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "engine_internal.h"
+#include "packing_launch.h"
+#include "paradmm.h"
+#include "paradmm_gpu.h"
+
+// ===========================================================================
+// Errors
+// ===========================================================================
+static thread_local int t_status = PARADMM_OK;
+static thread_local char t_msg[512] = "";
+
+int pdm_set_error(int status, const char *fmt, ...)
+{
+    t_status = status;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_msg, sizeof t_msg, fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+int pdm_cuda_fail(cudaError_t e, const char *what, const char *file, int line)
+{
+    int st = PARADMM_ECUDA;
+    if (e == cudaErrorMemoryAllocation) st = PARADMM_ENOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInvalidDevice) st = PARADMM_ENODEVICE;
+    cudaGetLastError();  // clear a sticky-free error so the next call starts clean
+    return pdm_set_error(st, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+
+extern "C" void paradmm_internal_set_error(int status, const char *msg) { pdm_set_error(status, "%s", msg); }
+extern "C" int paradmm_last_status(void) { return t_status; }
+extern "C" const char *paradmm_last_error_string(void) { return t_msg; }
+
+static inline void ok_status() { t_status = PARADMM_OK; }
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int d)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// ===========================================================================
+// Operator registry
+// ===========================================================================
+static std::mutex g_reg_mu;
+static std::vector<std::pair<void *, int>> g_reg;
+
+extern "C" int paradmm_gpu_register_op(paradmm_op_fn op, int kind)
+{
+    ok_status();
+    if (!op || kind < PARADMM_OP_PAIR || kind > PARADMM_OP_RADIUS)
+        return pdm_set_error(PARADMM_EINVAL, "paradmm_gpu_register_op: bad operator or kind %d", kind);
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    for (auto &p : g_reg)
+        if (p.first == (void *)op) { p.second = kind; return PARADMM_OK; }
+    g_reg.emplace_back((void *)op, kind);
+    return PARADMM_OK;
+}
+
+static int kind_of_name(const char *s)
+{
+    if (!s) return PARADMM_OP_UNKNOWN;
+    if (!strcmp(s, "disk_collision_variable_radius")) return PARADMM_OP_PAIR;
+    if (!strcmp(s, "disk_plane_collision_variable_radius")) return PARADMM_OP_WALL;
+    if (!strcmp(s, "maximize_sum_of_squared_disk_radii_alpha")) return PARADMM_OP_RADIUS;
+    return PARADMM_OP_UNKNOWN;
+}
+
+// Known by identity with this library's operators, by registration, or by
+// the exported symbol name of the function the pointer refers to (a caller's
+// own copy of a reference operator, e.g. packing/host.c compiled into a
+// shared object or an executable linked with -rdynamic).
+static int op_kind(paradmm_op_fn f)
+{
+    if (f == disk_collision_variable_radius) return PARADMM_OP_PAIR;
+    if (f == disk_plane_collision_variable_radius) return PARADMM_OP_WALL;
+    if (f == maximize_sum_of_squared_disk_radii_alpha) return PARADMM_OP_RADIUS;
+    {
+        std::lock_guard<std::mutex> lk(g_reg_mu);
+        for (auto &p : g_reg)
+            if (p.first == (void *)f) return p.second;
+    }
+    Dl_info info;
+    if (f && dladdr((void *)f, &info) && info.dli_saddr == (void *)f) return kind_of_name(info.dli_sname);
+    return PARADMM_OP_UNKNOWN;
+}
+
+// ===========================================================================
+// Graph analysis
+// ===========================================================================
+static int analyze_graph(const graph *G, GraphInfo &gi, bool need_state)
+{
+    if (!G) return pdm_set_error(PARADMM_EINVAL, "graph is NULL");
+    if (G->num_dims < 1 || G->num_edges < 1 || G->num_opts < 1 || G->num_vars < 1)
+        return pdm_set_error(PARADMM_EINVAL, "empty graph (%d factors, %d vars, %d edges, %d dims)", G->num_opts,
+                             G->num_vars, G->num_edges, G->num_dims);
+    if (!G->list_of_operators_functions_pointers || !G->operatorix_to_numedges || !G->operatorix_to_edgelistix ||
+        !G->varix_to_numedges || !G->varix_to_edgelistix || !G->edgeix_to_varlistix)
+        return pdm_set_error(PARADMM_EINVAL, "graph topology arrays are not built");
+    if (need_state && (!G->X || !G->M || !G->N || !G->U || !G->Z || !G->RHOS || !G->ALPHAS))
+        return pdm_set_error(PARADMM_EINVAL, "graph state is not initialised (call initialize_RHOS_APHAS and initialize_X_N_Z_M_U_*)");
+    const int d = G->num_dims;
+    gi.kind.assign(G->num_opts, PARADMM_OP_UNKNOWN);
+    long long edges_seen = 0;
+    for (int f = 0; f < G->num_opts; ++f) {
+        const int k = op_kind(G->list_of_operators_functions_pointers[f]);
+        if (k == PARADMM_OP_UNKNOWN)
+            return pdm_set_error(PARADMM_EUNSUPPORTED_OP,
+                                 "factor %d: operator %p is not one of the packing operators "
+                                 "(register the caller's copy with paradmm_gpu_register_op)",
+                                 f, (void *)G->list_of_operators_functions_pointers[f]);
+        const int nv = G->operatorix_to_numedges[f];
+        const int *el = G->operatorix_to_edgelistix[f];
+        if (nv < 1 || !el) return pdm_set_error(PARADMM_EINVAL, "factor %d has no edges", f);
+        for (int q = 0; q < nv; ++q)
+            if (el[q] != el[0] + q || el[q] < 0 || el[q] >= G->num_edges)
+                return pdm_set_error(PARADMM_EINVAL, "factor %d: edge ids are not a contiguous in-range slice", f);
+        edges_seen += nv;
+        void *prm = G->list_of_operators_param_pointers ? G->list_of_operators_param_pointers[f] : nullptr;
+        if (k == PARADMM_OP_PAIR && nv < 4) return pdm_set_error(PARADMM_EINVAL, "pair factor %d has %d edges (needs 4)", f, nv);
+        if (k == PARADMM_OP_WALL && (nv < 2 || !prm))
+            return pdm_set_error(PARADMM_EINVAL, "wall factor %d needs 2 edges and a [v, p] parameter block", f);
+        if (k == PARADMM_OP_RADIUS && !prm) return pdm_set_error(PARADMM_EINVAL, "radius factor %d has no exponent parameter", f);
+        gi.kind[f] = k;
+    }
+    if (edges_seen != G->num_edges) return pdm_set_error(PARADMM_EINVAL, "factor edge counts do not add up to num_edges");
+    for (int e = 0; e < G->num_edges; ++e)
+        if (G->edgeix_to_varlistix[e] < 0 || G->edgeix_to_varlistix[e] >= G->num_vars)
+            return pdm_set_error(PARADMM_EINVAL, "edge %d: variable index out of range", e);
+    gi.ok = 1;
+
+    // ---- packing structure ----
+    auto no = [&](const char *why) { gi.packing_ok = 0; gi.packing_why = why; return PARADMM_OK; };
+    if (d != 2) return no("num_dims is not 2");
+    const int V = G->num_vars;
+    std::vector<int> role(V, 0), partner(V, -1);  // role 1 centre, 2 radius
+    auto couple = [&](int c, int r) -> bool {
+        if (role[c] == 2 || role[r] == 1) return false;
+        if (role[c] == 1 && partner[c] != r) return false;
+        if (role[r] == 2 && partner[r] >= 0 && partner[r] != c) return false;
+        role[c] = 1; role[r] = 2; partner[c] = r; partner[r] = c;
+        return true;
+    };
+    long long npairs = 0;
+    for (int f = 0; f < G->num_opts; ++f) {
+        const int e0 = G->operatorix_to_edgelistix[f][0], nv = G->operatorix_to_numedges[f];
+        const int *ev = G->edgeix_to_varlistix + e0;
+        if (gi.kind[f] == PARADMM_OP_PAIR) {
+            if (nv != 4) return no("a pair factor has more than 4 edges");
+            if (!couple(ev[0], ev[1]) || !couple(ev[2], ev[3])) return no("variables do not form consistent (centre, radius) couples");
+            ++npairs;
+        } else if (gi.kind[f] == PARADMM_OP_WALL) {
+            if (nv != 2) return no("a wall factor has more than 2 edges");
+            if (!couple(ev[0], ev[1])) return no("variables do not form consistent (centre, radius) couples");
+        }
+    }
+    for (int f = 0; f < G->num_opts; ++f) {
+        if (gi.kind[f] != PARADMM_OP_RADIUS) continue;
+        const int e0 = G->operatorix_to_edgelistix[f][0], nv = G->operatorix_to_numedges[f];
+        for (int q = 0; q < nv; ++q) {
+            const int v = G->edgeix_to_varlistix[e0 + q];
+            if (role[v] != 2) return no("a radius factor acts on a variable that is not a circle's radius");
+        }
+    }
+    gi.circle_of_var.assign(V, -1);
+    gi.centre_var.clear();
+    gi.radius_var.clear();
+    for (int v = 0; v < V; ++v) {
+        if (role[v] == 0) return no("a variable has no pair or wall factor");
+        if (role[v] == 1) {
+            gi.circle_of_var[v] = (int)gi.centre_var.size();
+            gi.centre_var.push_back(v);
+            gi.radius_var.push_back(partner[v]);
+        }
+    }
+    for (int c = 0; c < (int)gi.centre_var.size(); ++c) gi.circle_of_var[gi.radius_var[c]] = c;
+    gi.N = (int)gi.centre_var.size();
+    if (gi.N < 2 || gi.N > 32767) return no("circle count outside [2, 32767]");
+    if (npairs != (long long)gi.N * (gi.N - 1) / 2) return no("not every pair of circles has exactly one pair factor");
+    std::vector<uint8_t> seen((size_t)gi.N * gi.N, 0);
+    double rho0[4] = {0, 0, 0, 0}, al0[4] = {0, 0, 0, 0};
+    bool first = true;
+    for (int f = 0; f < G->num_opts; ++f) {
+        if (gi.kind[f] != PARADMM_OP_PAIR) continue;
+        const int e0 = G->operatorix_to_edgelistix[f][0];
+        const int P = gi.circle_of_var[G->edgeix_to_varlistix[e0]], Q = gi.circle_of_var[G->edgeix_to_varlistix[e0 + 2]];
+        if (P >= Q) return no("pair factor circles out of order");
+        uint8_t &s = seen[(size_t)P * gi.N + Q];
+        if (s) return no("a pair of circles has two pair factors");
+        s = 1;
+        if (need_state) {
+            for (int q = 0; q < 4; ++q) {
+                if (first) { rho0[q] = G->RHOS[e0 + q]; al0[q] = G->ALPHAS[e0 + q]; }
+                else if (G->RHOS[e0 + q] != rho0[q] || G->ALPHAS[e0 + q] != al0[q])
+                    return no("pair-edge penalties or steps differ between pair factors");
+            }
+            first = false;
+        }
+    }
+    if (need_state) {
+        for (int e = 0; e < G->num_edges; ++e) {
+            const int v = G->edgeix_to_varlistix[e];
+            if (role[v] == 2 && (G->N[2LL * e] != G->N[2LL * e + 1] || G->U[2LL * e] != G->U[2LL * e + 1]))
+                return no("a radius edge holds two different components (N or U)");
+        }
+        for (int c = 0; c < gi.N; ++c) {
+            const int r = gi.radius_var[c];
+            if (G->Z[2LL * r] != G->Z[2LL * r + 1]) return no("a radius variable holds two different components (Z)");
+        }
+    }
+    gi.packing_ok = 1;
+    return PARADMM_OK;
+}
+
+// ===========================================================================
+// Device memory helpers
+// ===========================================================================
+static int dalloc(paradmm_gpu *h, void **p, size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return pdm_cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    h->allocs.push_back(*p);
+    h->device_bytes += (long long)bytes;
+    return PARADMM_OK;
+}
+
+template <class T>
+static int dput(paradmm_gpu *h, T **p, const std::vector<T> &v)
+{
+    int rc = dalloc(h, (void **)p, sizeof(T) * v.size());
+    if (rc) return rc;
+    if (!v.empty()) PDM_CUDA(cudaMemcpy(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return PARADMM_OK;
+}
+
+static void free_handle_memory(paradmm_gpu *h)
+{
+    for (void *p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    h->ev0 = h->ev1 = nullptr;
+    h->stream = nullptr;
+}
+
+static int handle_init(paradmm_gpu *h, const paradmm_gpu_opts *opts)
+{
+    if (opts) h->opts = *opts;
+    else paradmm_gpu_default_opts(&h->opts);
+    h->device = h->opts.device;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return pdm_set_error(PARADMM_ENODEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+    }
+    if (h->device < 0 || h->device >= ndev) return pdm_set_error(PARADMM_ENODEVICE, "device %d does not exist", h->device);
+    PDM_CUDA(cudaSetDevice(h->device));
+    PDM_CUDA(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+    int coop = 0;
+    PDM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device));
+    if (!coop) return pdm_set_error(PARADMM_ENODEVICE, "device %d cannot run cooperative launches", h->device);
+    PDM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    PDM_CUDA(cudaEventCreate(&h->ev0));
+    PDM_CUDA(cudaEventCreate(&h->ev1));
+    int rc = dalloc(h, (void **)&h->ctl, sizeof(DevCtl));
+    if (rc) return rc;
+    PDM_CUDA(cudaMemset(h->ctl, 0, sizeof(DevCtl)));
+    return PARADMM_OK;
+}
+
+extern "C" void paradmm_gpu_default_opts(paradmm_gpu_opts *o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof *o);
+    o->engine = PARADMM_ENGINE_AUTO;
+    o->check_every = 1;
+}
+
+// ===========================================================================
+// Packing engine: construction
+// ===========================================================================
+static void pair_coefficients(PkInst &I, const double rho[4], const double alpha[4])
+{
+    const double rx1 = rho[0], rr1 = rho[1], rx2 = rho[2], rr2 = rho[3];
+    const double den = rr1 * rr2 * rx1 + rr2 * rx1 * rx2 + rr1 * (rr2 + rx1) * rx2;
+    I.A1 = (float)(rr1 * rr2 * rx2 / den);
+    I.A2 = (float)(rr1 * rr2 * rx1 / den);
+    I.B2m1 = (float)((rr2 * rx1 + rr1 * (rr2 + rx1)) * rx2 / den - 1.0);
+    I.C1 = (float)(rr2 * rx1 * rx2 / den);
+    I.D1 = (float)(rr1 * (rx1 * rx2 + rr2 * (rx1 + rx2)) / den);
+    I.C2 = (float)(rr1 * rx1 * rx2 / den);
+    I.D2 = (float)(rr2 * (rx1 * rx2 + rr1 * (rx1 + rx2)) / den);
+    for (int q = 0; q < 4; ++q) { I.rho[q] = rho[q]; I.alpha[q] = (float)alpha[q]; }
+}
+
+// Work items of one instance: pair tiles then circle blocks.  Returns the
+// number added.
+static int add_items(PkHost &P, int inst_id, int N, int nb)
+{
+    int n = 0;
+    for (int I = 0; I < nb; ++I)
+        for (int J = I; J < nb; ++J) { P.items.push_back(make_int4(inst_id, 0, I, J)); ++n; }
+    for (int c0 = 0; c0 < N; c0 += PK_THREADS) { P.items.push_back(make_int4(inst_id, 1, c0, std::min(PK_THREADS, N - c0))); ++n; }
+    return n;
+}
+
+static int pick_V(const paradmm_gpu_opts &o, int maxN)
+{
+    if (o.block_width == 32) return 1;
+    if (o.block_width == 64) return 2;
+    if (o.block_width == 128) return 4;
+    if (maxN <= 160) return 1;
+    return 2;
+}
+
+// Allocates and uploads everything of a packing handle whose host tables
+// (inst, items, circ, walls, rads, init_Z) are filled.
+static int pk_finalize_build(paradmm_gpu *h)
+{
+    PkHost &P = *h->pk;
+    P.n_inst = (int)P.inst.size();
+    P.n_circ = (int)P.circ.size();
+    P.n_wall = (int)P.wall_vp.size();
+    P.n_rad = (int)P.rad_coef.size();
+    // Items are instance-major (the residual reduction reads each instance's
+    // items as one range); blocks claim them largest first so the dynamic
+    // schedule ends evenly.
+    P.n_items = (int)P.items.size();
+    std::vector<int> claim(P.n_items);
+    std::vector<long long> cost(P.n_items);
+    {
+        std::vector<int> base(P.n_inst + 1, 0);
+        for (int q = 0; q < P.n_items; ++q) {
+            const int4 &it = P.items[q];
+            base[it.x + 1]++;
+            const PkInst &I = P.inst[it.x];
+            if (it.y == 1) cost[q] = it.w;
+            else {
+                const int nI = std::min(P.BW, I.N - it.z * P.BW), nJ = std::min(P.BW, I.N - it.w * P.BW);
+                cost[q] = it.z == it.w ? (long long)nI * (nI - 1) / 2 : (long long)nI * nJ;
+            }
+            claim[q] = q;
+        }
+        for (int i = 0; i < P.n_inst; ++i) base[i + 1] += base[i];
+        for (int i = 0; i < P.n_inst; ++i) { P.inst[i].item_base = base[i]; P.inst[i].n_items = base[i + 1] - base[i]; }
+        std::stable_sort(claim.begin(), claim.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    }
+
+    PkDev &D = P.D;
+    D.n_inst = P.n_inst;
+    D.n_items = P.n_items;
+    D.n_circ = P.n_circ;
+    int rc;
+    if ((rc = dput(h, (PkInst **)&D.inst, P.inst))) return rc;
+    if ((rc = dput(h, (int4 **)&D.items, P.items))) return rc;
+    if ((rc = dput(h, (int **)&D.claim, claim))) return rc;
+    if ((rc = dput(h, (PkCircle **)&D.circ, P.circ))) return rc;
+    const long long tile_bytes = pk_tile_floats(P.BW) * 4LL;
+    if ((rc = dalloc(h, (void **)&D.tiles, (size_t)(P.n_tiles * tile_bytes)))) return rc;
+    if ((rc = dalloc(h, (void **)&D.row_part, sizeof(double4) * (size_t)P.n_tiles * P.BW))) return rc;
+    if ((rc = dalloc(h, (void **)&D.col_part, sizeof(double4) * (size_t)P.n_tiles * P.BW))) return rc;
+    {
+        std::vector<double4> z(P.n_circ);
+        for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(P.init_Z[3 * g], P.init_Z[3 * g + 1], P.init_Z[3 * g + 2], 0.0);
+        if ((rc = dput(h, &D.Z, z))) return rc;
+    }
+    if ((rc = dalloc(h, (void **)&D.local_part, sizeof(double4) * (size_t)P.n_circ))) return rc;
+    if ((rc = dalloc(h, (void **)&D.circ_dual, sizeof(double) * 2 * (size_t)P.n_circ))) return rc;
+    if ((rc = dalloc(h, (void **)&D.item_primal, sizeof(double) * 2 * (size_t)P.n_items))) return rc;
+    PDM_CUDA(cudaMemset(D.circ_dual, 0, sizeof(double) * 2 * (size_t)P.n_circ));
+    PDM_CUDA(cudaMemset(D.item_primal, 0, sizeof(double) * 2 * (size_t)P.n_items));
+    if ((rc = dalloc(h, (void **)&D.status, sizeof(PkStatus) * (size_t)P.n_inst))) return rc;
+    if ((rc = dput(h, (float4 **)&D.wall_vp, P.wall_vp))) return rc;
+    if ((rc = dput(h, (float4 **)&D.wall_coef, P.wall_coef))) return rc;
+    if ((rc = dput(h, (double2 **)&D.wall_rho, P.wall_rho))) return rc;
+    if ((rc = dalloc(h, (void **)&D.wall_X, sizeof(float4) * (size_t)std::max(P.n_wall, 1)))) return rc;
+    if ((rc = dalloc(h, (void **)&D.wall_U, sizeof(float4) * (size_t)std::max(P.n_wall, 1)))) return rc;
+    if ((rc = dput(h, (float4 **)&D.rad_coef, P.rad_coef))) return rc;
+    if ((rc = dput(h, (double **)&D.rad_rho, P.rad_rho))) return rc;
+    if ((rc = dalloc(h, (void **)&D.rad_XU, sizeof(float2) * (size_t)std::max(P.n_rad, 1)))) return rc;
+    if ((rc = dalloc(h, (void **)&P.d_viol, sizeof(unsigned long long) * (size_t)P.n_inst))) return rc;
+    if ((rc = dalloc(h, (void **)&P.d_flag, sizeof(int)))) return rc;
+    D.ctl = h->ctl;
+
+    // grid: co-resident blocks for the cooperative launch
+    int bps = 0;
+    if (pk_max_blocks_per_sm(P.V, P.stream_hint, &bps) != cudaSuccess || bps < 1)
+        return pdm_set_error(PARADMM_ECUDA, "packing kernel cannot be resident on this device");
+    if (h->opts.ctas_per_sm > 0) bps = std::min(bps, h->opts.ctas_per_sm);
+    P.grid = h->num_sms * bps;
+    P.upload_iter.assign(P.n_inst, 0);
+    P.nmode.assign(P.n_inst, 0);
+    P.status.assign(P.n_inst, PkStatus{});
+    for (auto &s : P.status) { s.resid_iter = -1; s.primal = s.dual = NAN; }
+    P.iters_last_call.assign(P.n_inst, 0);
+    return PARADMM_OK;
+}
+
+static int pk_init_instance_state(paradmm_gpu *h, int inst, const float *d_pair_duals)
+{
+    PkHost &P = *h->pk;
+    cudaError_t e = pk_launch_init(P.V, P.D, inst, d_pair_duals, h->num_sms * 4, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    P.nmode[inst] = 0;
+    P.upload_iter[inst] = P.it_next;
+    return PARADMM_OK;
+}
+
+// One instance of the structured packing problem (paradmm_packing_desc).
+static int pk_add_desc(PkHost &P, const paradmm_packing_desc &d, int inst_id)
+{
+    const int N = d.n_circles;
+    PkInst I{};
+    I.N = N;
+    I.nb = (N + P.BW - 1) / P.BW;
+    I.circle_base = (int)P.circ.size();
+    I.tile_base = P.n_tiles;
+    P.n_tiles += (long long)I.nb * (I.nb + 1) / 2;
+    const double rho[4] = {d.rho, d.rho, d.rho, d.rho}, al[4] = {d.alpha, d.alpha, d.alpha, d.alpha};
+    pair_coefficients(I, rho, al);
+    const long long E = (long long)N + 2LL * d.n_walls * N + 4LL * N * (N - 1) / 2;
+    I.inv_ncomp = 1.0 / (2.0 * (double)E);
+    P.wall_base.push_back((int)P.wall_vp.size());
+    P.rad_base.push_back((int)P.rad_coef.size());
+    for (int c = 0; c < N; ++c) {
+        PkCircle C{};
+        const double deg_c = (N - 1) + d.n_walls, deg_r = (N - 1) + d.n_walls + 1;
+        C.inv_rho_c = 1.0 / (d.rho * (N - 1) + d.rho * d.n_walls);
+        C.inv_rho_r = 1.0 / (d.rho * (N - 1) + d.rho * d.n_walls + d.rho_radius);
+        C.w_c = deg_c;
+        C.w_r = 2.0 * deg_r;
+        C.wall_start = (int)P.wall_vp.size();
+        C.wall_count = d.n_walls;
+        for (int w = 0; w < d.n_walls; ++w) {
+            const double *W = d.walls + 4 * w;
+            P.wall_vp.push_back(make_float4((float)W[0], (float)W[1], (float)W[2], (float)W[3]));
+            P.wall_coef.push_back(make_float4((float)d.rho, (float)d.rho, (float)d.alpha, (float)d.alpha));
+            P.wall_rho.push_back(make_double2(d.rho, d.rho));
+            P.wall_circle.push_back(c);
+        }
+        C.rad_start = (int)P.rad_coef.size();
+        C.rad_count = 1;
+        P.rad_coef.push_back(make_float4((float)d.exponent, (float)d.rho_radius, (float)d.alpha, 0.f));
+        P.rad_rho.push_back(d.rho_radius);
+        P.rad_circle.push_back(c);
+        C.inst = inst_id;
+        P.circ.push_back(C);
+        P.init_Z.push_back(d.init[3 * c]);
+        P.init_Z.push_back(d.init[3 * c + 1]);
+        P.init_Z.push_back(d.init[3 * c + 2]);
+    }
+    add_items(P, inst_id, N, I.nb);
+    P.inst.push_back(I);
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_create_packing(const paradmm_packing_desc *descs, int count, const paradmm_gpu_opts *opts,
+                                          paradmm_gpu **out)
+{
+    ok_status();
+    if (!out) return pdm_set_error(PARADMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!descs || count < 1) return pdm_set_error(PARADMM_EINVAL, "no packing instances");
+    int maxN = 0;
+    for (int i = 0; i < count; ++i) {
+        const paradmm_packing_desc &d = descs[i];
+        if (d.n_circles < 2 || d.n_circles > 32767 || d.n_walls < 0 || d.n_walls > 8 || (d.n_walls && !d.walls) || !d.init)
+            return pdm_set_error(PARADMM_EINVAL, "instance %d: bad description (n_circles %d, n_walls %d)", i, d.n_circles, d.n_walls);
+        if (!(d.rho > 0) || !(d.rho_radius > 0)) return pdm_set_error(PARADMM_EINVAL, "instance %d: penalties must be positive", i);
+        maxN = std::max(maxN, d.n_circles);
+    }
+    paradmm_gpu *h = new paradmm_gpu();
+    int rc = handle_init(h, opts);
+    if (rc) { free_handle_memory(h); delete h; return rc; }
+    DevGuard g(h->device);
+    if (h->opts.engine != PARADMM_ENGINE_AUTO && h->opts.engine != PARADMM_ENGINE_PACKING) {
+        free_handle_memory(h); delete h;
+        return pdm_set_error(PARADMM_EUNSUPPORTED_GRAPH, "structured packing problems run on the packing engine only");
+    }
+    h->engine = PARADMM_ENGINE_PACKING;
+    h->pk = new PkHost();
+    PkHost &P = *h->pk;
+    P.V = pick_V(h->opts, maxN);
+    P.BW = 32 * P.V;
+    P.stream_hint = true;
+    P.dynamic = 1;
+    for (int i = 0; i < count; ++i) pk_add_desc(P, descs[i], i);
+    rc = pk_finalize_build(h);
+    for (int i = 0; rc == PARADMM_OK && i < count; ++i) rc = pk_init_instance_state(h, i, nullptr);
+    if (rc) { free_handle_memory(h); delete h->pk; delete h; return rc; }
+    h->num_dims = 2;
+    *out = h;
+    return PARADMM_OK;
+}
+
+// Packing handle from a host graph (single instance).
+static int pk_build_from_graph(paradmm_gpu *h, const graph *G, const GraphInfo &gi)
+{
+    h->pk = new PkHost();
+    PkHost &P = *h->pk;
+    const int N = gi.N;
+    P.V = pick_V(h->opts, N);
+    P.BW = 32 * P.V;
+    PkInst I{};
+    I.N = N;
+    I.nb = (N + P.BW - 1) / P.BW;
+    I.circle_base = 0;
+    I.tile_base = 0;
+    P.n_tiles = (long long)I.nb * (I.nb + 1) / 2;
+    I.inv_ncomp = 1.0 / ((double)G->num_edges * G->num_dims);
+    // pair penalties/steps by position (uniform, checked by analyze_graph)
+    double rho[4] = {1, 1, 1, 1}, al[4] = {1, 1, 1, 1};
+    std::vector<int2> pmap;
+    pmap.reserve((size_t)N * (N - 1) / 2);
+    std::vector<std::vector<int>> walls_of(N), rads_of(N);
+    for (int f = 0; f < G->num_opts; ++f) {
+        const int e0 = G->operatorix_to_edgelistix[f][0];
+        if (gi.kind[f] == PARADMM_OP_PAIR) {
+            if (pmap.empty())
+                for (int q = 0; q < 4; ++q) { rho[q] = G->RHOS[e0 + q]; al[q] = G->ALPHAS[e0 + q]; }
+            const int Pc = gi.circle_of_var[G->edgeix_to_varlistix[e0]], Qc = gi.circle_of_var[G->edgeix_to_varlistix[e0 + 2]];
+            pmap.push_back(make_int2(e0, (Pc << 16) | Qc));
+        } else if (gi.kind[f] == PARADMM_OP_WALL) {
+            walls_of[gi.circle_of_var[G->edgeix_to_varlistix[e0]]].push_back(f);
+        } else {
+            const int nv = G->operatorix_to_numedges[f];
+            for (int q = 0; q < nv; ++q) rads_of[gi.circle_of_var[G->edgeix_to_varlistix[e0 + q]]].push_back(e0 + q);
+        }
+    }
+    pair_coefficients(I, rho, al);
+    std::vector<int> wmap, rmap;
+    std::vector<int2> cmap(N);
+    P.wall_base.push_back(0);
+    P.rad_base.push_back(0);
+    for (int c = 0; c < N; ++c) {
+        PkCircle C{};
+        const int cv = gi.centre_var[c], rv = gi.radius_var[c];
+        cmap[c] = make_int2(cv, rv);
+        double sc = 0, sr = 0;
+        for (int q = 0; q < G->varix_to_numedges[cv]; ++q) sc += G->RHOS[G->varix_to_edgelistix[cv][q]];
+        for (int q = 0; q < G->varix_to_numedges[rv]; ++q) sr += G->RHOS[G->varix_to_edgelistix[rv][q]];
+        C.inv_rho_c = 1.0 / sc;
+        C.inv_rho_r = 1.0 / sr;
+        C.w_c = G->varix_to_numedges[cv];
+        C.w_r = 2.0 * G->varix_to_numedges[rv];
+        C.wall_start = (int)P.wall_vp.size();
+        C.wall_count = (int)walls_of[c].size();
+        for (int f : walls_of[c]) {
+            const int e0 = G->operatorix_to_edgelistix[f][0];
+            const double *W = (const double *)G->list_of_operators_param_pointers[f];
+            P.wall_vp.push_back(make_float4((float)W[0], (float)W[1], (float)W[2], (float)W[3]));
+            P.wall_coef.push_back(make_float4((float)G->RHOS[e0], (float)G->RHOS[e0 + 1], (float)G->ALPHAS[e0], (float)G->ALPHAS[e0 + 1]));
+            P.wall_rho.push_back(make_double2(G->RHOS[e0], G->RHOS[e0 + 1]));
+            P.wall_circle.push_back(c);
+            wmap.push_back(e0);
+        }
+        C.rad_start = (int)P.rad_coef.size();
+        C.rad_count = (int)rads_of[c].size();
+        for (int e : rads_of[c]) {
+            // exponent filled in below from the owning factor's params[0]
+            P.rad_coef.push_back(make_float4(0.f, (float)G->RHOS[e], (float)G->ALPHAS[e], 0.f));
+            P.rad_rho.push_back(G->RHOS[e]);
+            P.rad_circle.push_back(c);
+            rmap.push_back(e);
+        }
+        C.inst = 0;
+        P.circ.push_back(C);
+        P.init_Z.push_back(G->Z[2LL * cv]);
+        P.init_Z.push_back(G->Z[2LL * cv + 1]);
+        P.init_Z.push_back(G->Z[2LL * rv]);
+    }
+    // exponents of the radius factors, by edge
+    {
+        std::unordered_map<int, float> expo;
+        for (int f = 0; f < G->num_opts; ++f)
+            if (gi.kind[f] == PARADMM_OP_RADIUS) {
+                const int e0 = G->operatorix_to_edgelistix[f][0], nv = G->operatorix_to_numedges[f];
+                const float a = (float)((const double *)G->list_of_operators_param_pointers[f])[0];
+                for (int q = 0; q < nv; ++q) expo[e0 + q] = a;
+            }
+        for (size_t q = 0; q < rmap.size(); ++q) P.rad_coef[q].x = expo[rmap[q]];
+    }
+    add_items(P, 0, N, I.nb);
+    P.inst.push_back(I);
+    int rc = pk_finalize_build(h);
+    if (rc) return rc;
+    P.n_pmap = (long long)pmap.size();
+    if ((rc = dput(h, &P.d_pmap, pmap))) return rc;
+    if ((rc = dput(h, &P.d_wmap, wmap))) return rc;
+    if ((rc = dput(h, &P.d_rmap, rmap))) return rc;
+    if ((rc = dput(h, &P.d_cmap, cmap))) return rc;
+    if ((rc = dput(h, &P.d_wcirc, P.wall_circle))) return rc;
+    if ((rc = dput(h, &P.d_rcirc, P.rad_circle))) return rc;
+    return PARADMM_OK;
+}
+
+// Reference-layout staging buffers on the device (allocated on first use).
+static int ensure_stage(paradmm_gpu *h)
+{
+    if (h->d_stage[0]) return PARADMM_OK;
+    const size_t ne = (size_t)h->num_edges * h->num_dims, nz = (size_t)h->num_vars * h->num_dims;
+    for (int q = 0; q < 4; ++q) {
+        int rc = dalloc(h, (void **)&h->d_stage[q], sizeof(double) * ne);
+        if (rc) return rc;
+    }
+    return dalloc(h, (void **)&h->d_stage[4], sizeof(double) * nz);
+}
+
+static int pk_upload_graph(paradmm_gpu *h, const graph *G)
+{
+    PkHost &P = *h->pk;
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const size_t ne = (size_t)h->num_edges * 2, nz = (size_t)h->num_vars * 2;
+    PDM_CUDA(cudaMemcpyAsync(h->d_stage[2], G->N, sizeof(double) * ne, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(h->d_stage[3], G->U, sizeof(double) * ne, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(h->d_stage[4], G->Z, sizeof(double) * nz, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemsetAsync(P.d_flag, 0, sizeof(int), h->stream));
+    cudaError_t e = pk_launch_scatter(P.V, P.D, 0, P.d_pmap, P.n_pmap, P.d_wmap, 0, P.n_wall, P.d_rmap, 0, P.n_rad,
+                                      P.d_cmap, h->d_stage[2], h->d_stage[3], h->d_stage[4], P.d_flag,
+                                      h->num_sms * 8, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_scatter", __FILE__, __LINE__);
+    int flag = 0;
+    PDM_CUDA(cudaMemcpyAsync(&flag, P.d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    if (flag)
+        return pdm_set_error(PARADMM_EUNSUPPORTED_GRAPH,
+                             "the uploaded state has radius edges whose two components differ; "
+                             "the packing engine keeps one (use PARADMM_ENGINE_GENERIC_F64)");
+    P.nmode[0] = 1;
+    P.upload_iter[0] = P.it_next;
+    return PARADMM_OK;
+}
+
+static int pk_download_graph(paradmm_gpu *h, graph *G)
+{
+    PkHost &P = *h->pk;
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const int nm = P.nmode[0];
+    cudaError_t e = pk_launch_gather(P.V, P.D, 0, P.d_pmap, P.n_pmap, P.d_wmap, 0, P.n_wall, P.d_rmap, 0, P.n_rad,
+                                     P.d_cmap, P.d_wcirc, P.d_rcirc, nm, h->d_stage[0], h->d_stage[1], h->d_stage[2],
+                                     h->d_stage[3], h->d_stage[4], h->num_sms * 8, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_gather", __FILE__, __LINE__);
+    const size_t ne = (size_t)h->num_edges * 2, nz = (size_t)h->num_vars * 2;
+    double *dst[5] = {G->X, G->M, G->N, G->U, G->Z};
+    for (int q = 0; q < 5; ++q) {
+        if (nm && q < 2) continue;  // no sweep since the upload: X and M are the caller's
+        PDM_CUDA(cudaMemcpyAsync(dst[q], h->d_stage[q], sizeof(double) * (q == 4 ? nz : ne), cudaMemcpyDeviceToHost, h->stream));
+    }
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    return PARADMM_OK;
+}
+
+// Runs up to n sweeps of every instance (persistent launches of at most
+// PK_SWEEPS_PER_LAUNCH sweeps).  Per-instance iteration counts land in
+// P.iters_last_call, statuses in P.status.
+#define PK_SWEEPS_PER_LAUNCH 8192
+static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, double *ms)
+{
+    PkHost &P = *h->pk;
+    std::fill(P.iters_last_call.begin(), P.iters_last_call.end(), 0LL);
+    std::vector<char> done(P.n_inst, 0);
+    double total_ms = 0;
+    long long left = n;
+    int rc = PARADMM_OK;
+    while (left > 0) {
+        const int chunk = (int)std::min<long long>(left, PK_SWEEPS_PER_LAUNCH);
+        const long long it0 = P.it_next;
+        int active = 0;
+        std::vector<PkStatus> st(P.n_inst);
+        for (int i = 0; i < P.n_inst; ++i) {
+            PkStatus &s = st[i];
+            s = P.status[i];
+            s.last_iter = done[i] ? it0 - 1 : LLONG_MAX;
+            s.check_from = it0 + 1;
+            s.converged = 0;
+            s.nonfinite = 0;
+            s.nmode = P.nmode[i];
+            if (!done[i]) ++active;
+        }
+        if (active == 0) break;
+        PDM_CUDA(cudaMemcpyAsync(P.D.status, st.data(), sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
+        DevCtl c{};
+        c.n_active = active;
+        PDM_CUDA(cudaMemcpyAsync(h->ctl, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
+        PkRun R{};
+        R.it0 = it0;
+        R.n_iter = chunk;
+        R.dynamic = P.dynamic;
+        R.tol = tol;
+        R.check_every = check_every < 1 ? 1 : check_every;
+        PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
+        cudaError_t e = pk_launch_persistent(P.V, P.stream_hint, P.D, R, P.grid, h->stream);
+        if (e != cudaSuccess) return pdm_cuda_fail(e, "packing persistent launch", __FILE__, __LINE__);
+        PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
+        PDM_CUDA(cudaMemcpyAsync(&c, h->ctl, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+        PDM_CUDA(cudaMemcpyAsync(st.data(), P.D.status, sizeof(PkStatus) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
+        PDM_CUDA(cudaStreamSynchronize(h->stream));
+        float t = 0;
+        cudaEventElapsedTime(&t, h->ev0, h->ev1);
+        total_ms += t;
+        if (c.err != DEV_OK)
+            return pdm_set_error(PARADMM_ETIMEOUT, "packing kernel: a grid barrier wait ran out (device error %d)", c.err);
+        const long long sweeps = (long long)c.pad[0];
+        for (int i = 0; i < P.n_inst; ++i) {
+            if (done[i]) continue;
+            const long long last = std::min(st[i].last_iter, it0 + sweeps - 1);
+            const long long ran = last - it0 + 1;
+            if (ran > 0) { P.iters_last_call[i] += ran; P.nmode[i] = 0; }
+            P.status[i] = st[i];
+            if (st[i].converged || st[i].nonfinite) done[i] = 1;
+            if (st[i].nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
+        }
+        P.it_next = it0 + sweeps;
+        left -= sweeps;
+        if (sweeps < chunk) break;  // every instance stopped
+    }
+    if (ms) *ms = total_ms;
+    return rc;
+}
+
+// ===========================================================================
+// Generic engine
+// ===========================================================================
+static int gen_build(paradmm_gpu *h, const graph *G, const GraphInfo &gi, bool fp64)
+{
+    h->gen = new GenHost();
+    GenHost &Gh = *h->gen;
+    GenDev &D = Gh.D;
+    const int d = G->num_dims;
+    D.num_dims = d;
+    D.num_vars = G->num_vars;
+    D.num_edges = G->num_edges;
+    D.num_opts = G->num_opts;
+    D.fp64 = fp64 ? 1 : 0;
+    std::vector<int> kind(gi.kind), nv(G->num_opts);
+    std::vector<long long> e0(G->num_opts), prm_off(G->num_opts, -1);
+    std::vector<double> params;
+    for (int f = 0; f < G->num_opts; ++f) {
+        e0[f] = G->operatorix_to_edgelistix[f][0];
+        nv[f] = G->operatorix_to_numedges[f];
+        const double *p = G->list_of_operators_param_pointers ? (const double *)G->list_of_operators_param_pointers[f] : nullptr;
+        if (kind[f] == PARADMM_OP_WALL) { prm_off[f] = (long long)params.size(); params.insert(params.end(), p, p + 2 * d); }
+        if (kind[f] == PARADMM_OP_RADIUS) { prm_off[f] = (long long)params.size(); params.push_back(p[0]); }
+    }
+    std::vector<int> e2v(G->edgeix_to_varlistix, G->edgeix_to_varlistix + G->num_edges);
+    std::vector<long long> voff(G->num_vars + 1, 0);
+    for (int v = 0; v < G->num_vars; ++v) voff[v + 1] = voff[v] + G->varix_to_numedges[v];
+    std::vector<int> vedges((size_t)voff[G->num_vars]);
+    for (int v = 0; v < G->num_vars; ++v)
+        std::copy(G->varix_to_edgelistix[v], G->varix_to_edgelistix[v] + G->varix_to_numedges[v], vedges.begin() + voff[v]);
+    int rc;
+    if ((rc = dput(h, (int **)&D.f_kind, kind))) return rc;
+    if ((rc = dput(h, (long long **)&D.f_e0, e0))) return rc;
+    if ((rc = dput(h, (int **)&D.f_nv, nv))) return rc;
+    if ((rc = dput(h, (long long **)&D.f_param, prm_off))) return rc;
+    if ((rc = dput(h, (double **)&D.params, params))) return rc;
+    if ((rc = dput(h, (int **)&D.e2v, e2v))) return rc;
+    if ((rc = dput(h, (long long **)&D.v_off, voff))) return rc;
+    if ((rc = dput(h, (int **)&D.v_edges, vedges))) return rc;
+    const size_t ne = (size_t)G->num_edges * d, nz = (size_t)G->num_vars * d;
+    const size_t ts = fp64 ? sizeof(double) : sizeof(float);
+    if ((rc = dalloc(h, &D.X, ts * ne)) || (rc = dalloc(h, &D.M, ts * ne)) || (rc = dalloc(h, &D.N, ts * ne)) ||
+        (rc = dalloc(h, &D.U, ts * ne)))
+        return rc;
+    if ((rc = dalloc(h, (void **)&D.Z, sizeof(double) * nz))) return rc;
+    if ((rc = dalloc(h, (void **)&Gh.d_Zprev, sizeof(double) * nz))) return rc;
+    if ((rc = dalloc(h, (void **)&D.RHOS, sizeof(double) * G->num_edges))) return rc;
+    if ((rc = dalloc(h, (void **)&D.ALPHAS, sizeof(double) * G->num_edges))) return rc;
+    if ((rc = dalloc(h, (void **)&Gh.d_acc, sizeof(double) * 2))) return rc;
+    if ((rc = dalloc(h, (void **)&Gh.d_viol, sizeof(unsigned long long)))) return rc;
+    if (gi.packing_ok)
+        for (int c = 0; c < gi.N; ++c) Gh.radius_vars.push_back(gi.radius_var[c]);
+    return PARADMM_OK;
+}
+
+static int gen_upload(paradmm_gpu *h, const graph *G)
+{
+    GenHost &Gh = *h->gen;
+    GenDev &D = Gh.D;
+    const size_t ne = (size_t)G->num_edges * G->num_dims, nz = (size_t)G->num_vars * G->num_dims;
+    const double *src[4] = {G->X, G->M, G->N, G->U};
+    void *dst[4] = {D.X, D.M, D.N, D.U};
+    if (D.fp64) {
+        for (int q = 0; q < 4; ++q) PDM_CUDA(cudaMemcpyAsync(dst[q], src[q], sizeof(double) * ne, cudaMemcpyHostToDevice, h->stream));
+    } else {
+        std::vector<float> tmp(ne);
+        for (int q = 0; q < 4; ++q) {
+            for (size_t i = 0; i < ne; ++i) tmp[i] = (float)src[q][i];
+            PDM_CUDA(cudaMemcpyAsync(dst[q], tmp.data(), sizeof(float) * ne, cudaMemcpyHostToDevice, h->stream));
+            PDM_CUDA(cudaStreamSynchronize(h->stream));
+        }
+    }
+    PDM_CUDA(cudaMemcpyAsync(D.Z, G->Z, sizeof(double) * nz, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemcpyAsync((void *)D.RHOS, G->RHOS, sizeof(double) * G->num_edges, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemcpyAsync((void *)D.ALPHAS, G->ALPHAS, sizeof(double) * G->num_edges, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    Gh.zprev_valid = 0;
+    return PARADMM_OK;
+}
+
+static int gen_download(paradmm_gpu *h, graph *G)
+{
+    GenDev &D = h->gen->D;
+    const size_t ne = (size_t)G->num_edges * G->num_dims, nz = (size_t)G->num_vars * G->num_dims;
+    double *dst[4] = {G->X, G->M, G->N, G->U};
+    const void *src[4] = {D.X, D.M, D.N, D.U};
+    if (D.fp64) {
+        for (int q = 0; q < 4; ++q) PDM_CUDA(cudaMemcpyAsync(dst[q], src[q], sizeof(double) * ne, cudaMemcpyDeviceToHost, h->stream));
+        PDM_CUDA(cudaMemcpyAsync(G->Z, D.Z, sizeof(double) * nz, cudaMemcpyDeviceToHost, h->stream));
+        PDM_CUDA(cudaStreamSynchronize(h->stream));
+    } else {
+        std::vector<float> tmp(ne);
+        for (int q = 0; q < 4; ++q) {
+            PDM_CUDA(cudaMemcpyAsync(tmp.data(), src[q], sizeof(float) * ne, cudaMemcpyDeviceToHost, h->stream));
+            PDM_CUDA(cudaStreamSynchronize(h->stream));
+            for (size_t i = 0; i < ne; ++i) dst[q][i] = (double)tmp[i];
+        }
+        PDM_CUDA(cudaMemcpyAsync(G->Z, D.Z, sizeof(double) * nz, cudaMemcpyDeviceToHost, h->stream));
+        PDM_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return PARADMM_OK;
+}
+
+static int gen_phase(paradmm_gpu *h, int phase)
+{
+    cudaError_t e = gen_launch_phase(h->gen->D, phase, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "generic phase kernel", __FILE__, __LINE__);
+    return PARADMM_OK;
+}
+
+static int gen_sweep(paradmm_gpu *h)
+{
+    int rc;
+    if ((rc = gen_phase(h, GEN_PHASE_XM)) || (rc = gen_phase(h, GEN_PHASE_Z)) || (rc = gen_phase(h, GEN_PHASE_UN))) return rc;
+    return PARADMM_OK;
+}
+
+static int gen_residuals(paradmm_gpu *h, double *primal, double *dual)
+{
+    GenHost &Gh = *h->gen;
+    PDM_CUDA(cudaMemsetAsync(Gh.d_acc, 0, sizeof(double) * 2, h->stream));
+    cudaError_t e = gen_launch_resid(Gh.D, Gh.zprev_valid ? Gh.d_Zprev : nullptr, Gh.d_acc, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "generic residual kernel", __FILE__, __LINE__);
+    double acc[2];
+    PDM_CUDA(cudaMemcpyAsync(acc, Gh.d_acc, sizeof acc, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    const double n = (double)Gh.D.num_edges * Gh.D.num_dims;
+    *primal = std::sqrt(acc[0] / n);
+    *dual = Gh.zprev_valid ? std::sqrt(acc[1] / n) : NAN;
+    return PARADMM_OK;
+}
+
+static int gen_run(paradmm_gpu *h, long long n, double tol, int check_every, paradmm_stats *stats)
+{
+    GenHost &Gh = *h->gen;
+    const size_t nz = (size_t)Gh.D.num_vars * Gh.D.num_dims;
+    if (check_every < 1) check_every = 1;
+    PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
+    long long done = 0;
+    int converged = 0, rc = PARADMM_OK;
+    double rp = NAN, rd = NAN;
+    while (done < n) {
+        const bool check = tol >= 0 && ((done + 1) % check_every == 0 || done + 1 == n);
+        if (check || done + 1 == n) {
+            PDM_CUDA(cudaMemcpyAsync(Gh.d_Zprev, Gh.D.Z, sizeof(double) * nz, cudaMemcpyDeviceToDevice, h->stream));
+            Gh.zprev_valid = 1;
+        }
+        if ((rc = gen_sweep(h))) return rc;
+        ++done;
+        if (check) {
+            if ((rc = gen_residuals(h, &rp, &rd))) return rc;
+            if (!std::isfinite(rp + rd)) { rc = pdm_set_error(PARADMM_ENONFINITE, "residual became NaN/Inf"); break; }
+            if (rp + rd <= tol) { converged = 1; break; }
+        }
+    }
+    PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    Gh.last_primal = rp;
+    Gh.last_dual = rd;
+    if (stats) {
+        stats->iterations = done;
+        stats->converged = converged;
+        stats->status = rc;
+        stats->primal = rp;
+        stats->dual = rd;
+        stats->device_ms = ms;
+    }
+    return rc;
+}
+
+// ===========================================================================
+// Public C-ABI
+// ===========================================================================
+extern "C" int paradmm_gpu_create(const graph *G, const paradmm_gpu_opts *opts, paradmm_gpu **out)
+{
+    ok_status();
+    if (!out) return pdm_set_error(PARADMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    GraphInfo gi;
+    int rc = analyze_graph(G, gi, true);
+    if (rc) return rc;
+    paradmm_gpu *h = new paradmm_gpu();
+    rc = handle_init(h, opts);
+    if (rc) { free_handle_memory(h); delete h; return rc; }
+    DevGuard guard(h->device);
+    h->from_graph = 1;
+    h->num_dims = G->num_dims;
+    h->num_vars = G->num_vars;
+    h->num_edges = G->num_edges;
+    h->num_opts = G->num_opts;
+    int eng = h->opts.engine;
+    if (eng == PARADMM_ENGINE_PACKING && !gi.packing_ok) {
+        free_handle_memory(h); delete h;
+        return pdm_set_error(PARADMM_EUNSUPPORTED_GRAPH, "packing engine: %s", gi.packing_why.c_str());
+    }
+    if (eng == PARADMM_ENGINE_AUTO) eng = gi.packing_ok ? PARADMM_ENGINE_PACKING : PARADMM_ENGINE_GENERIC_F64;
+    h->engine = eng;
+    if (eng == PARADMM_ENGINE_PACKING) {
+        rc = pk_build_from_graph(h, G, gi);
+        if (!rc) rc = pk_upload_graph(h, G);
+    } else {
+        rc = gen_build(h, G, gi, eng == PARADMM_ENGINE_GENERIC_F64);
+        if (!rc) rc = gen_upload(h, G);
+    }
+    if (rc) {
+        free_handle_memory(h);
+        delete h->pk;
+        delete h->gen;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return PARADMM_OK;
+}
+
+static bool same_topology(const paradmm_gpu *h, const graph *G)
+{
+    return G && h->from_graph && G->num_dims == h->num_dims && G->num_vars == h->num_vars && G->num_edges == h->num_edges &&
+           G->num_opts == h->num_opts;
+}
+
+extern "C" int paradmm_gpu_upload(paradmm_gpu *h, const graph *G)
+{
+    ok_status();
+    if (!h) return pdm_set_error(PARADMM_EINVAL, "handle is NULL");
+    if (!same_topology(h, G)) return pdm_set_error(PARADMM_EINVAL, "graph does not match the handle's topology");
+    if (!G->X || !G->M || !G->N || !G->U || !G->Z || !G->RHOS || !G->ALPHAS) return pdm_set_error(PARADMM_EINVAL, "graph state is not initialised");
+    DevGuard guard(h->device);
+    return h->engine == PARADMM_ENGINE_PACKING ? pk_upload_graph(h, G) : gen_upload(h, G);
+}
+
+extern "C" int paradmm_gpu_download(paradmm_gpu *h, graph *G)
+{
+    ok_status();
+    if (!h) return pdm_set_error(PARADMM_EINVAL, "handle is NULL");
+    if (!same_topology(h, G)) return pdm_set_error(PARADMM_EINVAL, "graph does not match the handle's topology");
+    if (!G->X || !G->M || !G->N || !G->U || !G->Z) return pdm_set_error(PARADMM_EINVAL, "graph state arrays are not allocated");
+    DevGuard guard(h->device);
+    return h->engine == PARADMM_ENGINE_PACKING ? pk_download_graph(h, G) : gen_download(h, G);
+}
+
+extern "C" int paradmm_gpu_solve(paradmm_gpu *h, int maxiter, double tol, paradmm_stats *stats)
+{
+    ok_status();
+    if (!h) return pdm_set_error(PARADMM_EINVAL, "handle is NULL");
+    if (maxiter < 0) return pdm_set_error(PARADMM_EINVAL, "maxiter < 0");
+    DevGuard guard(h->device);
+    if (stats) memset(stats, 0, sizeof *stats);
+    if (maxiter == 0) return PARADMM_OK;
+    if (h->engine != PARADMM_ENGINE_PACKING) return gen_run(h, maxiter, tol, h->opts.check_every, stats);
+    double ms = 0;
+    const int rc = pk_run(h, maxiter, tol, h->opts.check_every, &ms);
+    if (stats) {
+        PkHost &P = *h->pk;
+        long long it = 0;
+        int conv = 1;
+        double rp = 0, rd = 0;
+        for (int i = 0; i < P.n_inst; ++i) {
+            it = std::max(it, P.iters_last_call[i]);
+            conv &= P.status[i].converged;
+            rp = std::max(rp, P.status[i].primal);
+            rd = std::max(rd, P.status[i].dual);
+        }
+        stats->iterations = it;
+        stats->converged = conv;
+        stats->status = rc;
+        stats->primal = rp;
+        stats->dual = rd;
+        stats->device_ms = ms;
+        stats->max_violation = NAN;
+        stats->total_radius = NAN;
+    }
+    return rc;
+}
+
+extern "C" int paradmm_gpu_iterate(paradmm_gpu *h, int n) { return paradmm_gpu_solve(h, n, -1.0, nullptr); }
+
+// Max violation per instance (device) and total radius (host, from Z).
+static int pk_metrics(paradmm_gpu *h, std::vector<double> &viol, std::vector<double> &total)
+{
+    PkHost &P = *h->pk;
+    PDM_CUDA(cudaMemsetAsync(P.d_viol, 0, sizeof(unsigned long long) * P.n_inst, h->stream));
+    cudaError_t e = pk_launch_violation(P.D, P.d_viol, h->num_sms * 8, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_violation", __FILE__, __LINE__);
+    std::vector<unsigned long long> vb(P.n_inst);
+    std::vector<double4> z(P.n_circ);
+    PDM_CUDA(cudaMemcpyAsync(vb.data(), P.d_viol, sizeof(unsigned long long) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(z.data(), P.D.Z, sizeof(double4) * P.n_circ, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    viol.resize(P.n_inst);
+    total.assign(P.n_inst, 0.0);
+    for (int i = 0; i < P.n_inst; ++i) memcpy(&viol[i], &vb[i], sizeof(double));
+    for (int g = 0; g < P.n_circ; ++g) total[P.circ[g].inst] += z[g].z;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_instance_stats(paradmm_gpu *h, paradmm_stats *stats)
+{
+    ok_status();
+    if (!h || !stats) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    DevGuard guard(h->device);
+    if (h->engine != PARADMM_ENGINE_PACKING) return paradmm_gpu_stats(h, stats);
+    PkHost &P = *h->pk;
+    std::vector<double> viol, total;
+    int rc = pk_metrics(h, viol, total);
+    if (rc) return rc;
+    for (int i = 0; i < P.n_inst; ++i) {
+        paradmm_stats &s = stats[i];
+        memset(&s, 0, sizeof s);
+        s.iterations = P.iters_last_call[i];
+        s.converged = P.status[i].converged;
+        s.status = P.status[i].nonfinite ? PARADMM_ENONFINITE : PARADMM_OK;
+        s.primal = P.status[i].resid_iter >= 0 ? P.status[i].primal : NAN;
+        s.dual = P.status[i].resid_iter >= 0 ? P.status[i].dual : NAN;
+        s.max_violation = viol[i];
+        s.total_radius = total[i];
+    }
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_stats(paradmm_gpu *h, paradmm_stats *out)
+{
+    ok_status();
+    if (!h || !out) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    DevGuard guard(h->device);
+    if (h->engine == PARADMM_ENGINE_PACKING) {
+        if (h->pk->n_inst != 1) return pdm_set_error(PARADMM_EINVAL, "handle has %d instances: use paradmm_gpu_instance_stats", h->pk->n_inst);
+        return paradmm_gpu_instance_stats(h, out);
+    }
+    GenHost &Gh = *h->gen;
+    memset(out, 0, sizeof *out);
+    int rc = gen_residuals(h, &out->primal, &out->dual);
+    if (rc) return rc;
+    PDM_CUDA(cudaMemsetAsync(Gh.d_viol, 0, sizeof(unsigned long long), h->stream));
+    cudaError_t e = gen_launch_violation(Gh.D, Gh.d_viol, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "gen_violation", __FILE__, __LINE__);
+    unsigned long long vb = 0;
+    std::vector<double> z((size_t)Gh.D.num_vars * Gh.D.num_dims);
+    PDM_CUDA(cudaMemcpyAsync(&vb, Gh.d_viol, sizeof vb, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(z.data(), Gh.D.Z, sizeof(double) * z.size(), cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    memcpy(&out->max_violation, &vb, sizeof(double));
+    double tot = 0;
+    for (int v : Gh.radius_vars) tot += z[(size_t)v * Gh.D.num_dims];
+    out->total_radius = Gh.radius_vars.empty() ? NAN : tot;
+    out->converged = 0;
+    out->status = PARADMM_OK;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_engine(const paradmm_gpu *h) { return h ? h->engine : PARADMM_EINVAL; }
+extern "C" int paradmm_gpu_instances(const paradmm_gpu *h) { return !h ? 0 : (h->pk ? h->pk->n_inst : 1); }
+extern "C" int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h) { return h ? h->device_bytes : 0; }
+
+extern "C" int paradmm_gpu_get_circles(paradmm_gpu *h, int instance, double *out)
+{
+    ok_status();
+    if (!h || !out) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
+    PkHost &P = *h->pk;
+    if (instance < 0 || instance >= P.n_inst) return pdm_set_error(PARADMM_EINVAL, "instance %d out of range", instance);
+    DevGuard guard(h->device);
+    const PkInst &I = P.inst[instance];
+    std::vector<double4> z(I.N);
+    PDM_CUDA(cudaMemcpyAsync(z.data(), P.D.Z + I.circle_base, sizeof(double4) * I.N, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < I.N; ++c) { out[3 * c] = z[c].x; out[3 * c + 1] = z[c].y; out[3 * c + 2] = z[c].z; }
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double *circles, const float *pair_duals)
+{
+    ok_status();
+    if (!h || !circles) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
+    PkHost &P = *h->pk;
+    if (instance < 0 || instance >= P.n_inst) return pdm_set_error(PARADMM_EINVAL, "instance %d out of range", instance);
+    DevGuard guard(h->device);
+    const PkInst &I = P.inst[instance];
+    std::vector<double4> z(I.N);
+    for (int c = 0; c < I.N; ++c) z[c] = make_double4(circles[3 * c], circles[3 * c + 1], circles[3 * c + 2], 0.0);
+    PDM_CUDA(cudaMemcpyAsync(P.D.Z + I.circle_base, z.data(), sizeof(double4) * I.N, cudaMemcpyHostToDevice, h->stream));
+    float *d_du = nullptr;
+    const size_t nd = (size_t)I.N * (I.N - 1) / 2 * 6;
+    if (pair_duals) {
+        PDM_CUDA(cudaMalloc(&d_du, sizeof(float) * nd));
+        cudaError_t e = cudaMemcpyAsync(d_du, pair_duals, sizeof(float) * nd, cudaMemcpyHostToDevice, h->stream);
+        if (e != cudaSuccess) { cudaFree(d_du); return pdm_cuda_fail(e, "cudaMemcpyAsync", __FILE__, __LINE__); }
+    }
+    int rc = pk_init_instance_state(h, instance, d_du);
+    if (d_du) cudaFree(d_du);
+    return rc;
+}
+
+extern "C" void paradmm_gpu_destroy(paradmm_gpu *h)
+{
+    if (!h) return;
+    {
+        DevGuard guard(h->device);
+        free_handle_memory(h);
+    }
+    delete h->pk;
+    delete h->gen;
+    delete h;
+}
+
+// ===========================================================================
+// paradmm.h sweep functions (GPU-backed drop-ins)
+// ===========================================================================
+static std::mutex g_sweep_mu;
+static paradmm_gpu_opts g_sweep_opts = {0, PARADMM_ENGINE_AUTO, 0, 0, 1, {0}};
+
+struct Cached {
+    paradmm_gpu *h = nullptr;
+    int engine_req = 0;
+    int num_opts = 0, num_vars = 0, num_edges = 0, num_dims = 0;
+    const void *ptrs[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t coef_hash = 0;
+};
+static std::unordered_map<const graph *, std::vector<Cached>> g_cache;
+
+extern "C" void paradmm_set_sweep_options(const paradmm_gpu_opts *opts)
+{
+    std::lock_guard<std::mutex> lk(g_sweep_mu);
+    if (opts) g_sweep_opts = *opts;
+    else paradmm_gpu_default_opts(&g_sweep_opts);
+}
+
+static uint64_t coef_hash(const graph *G)
+{
+    uint64_t hsh = 1469598103934665603ULL;
+    auto mix = [&](const double *a, int n) {
+        for (int i = 0; i < n; ++i) {
+            uint64_t b;
+            memcpy(&b, &a[i], 8);
+            hsh = (hsh ^ b) * 1099511628211ULL;
+        }
+    };
+    if (G->RHOS) mix(G->RHOS, G->num_edges);
+    if (G->ALPHAS) mix(G->ALPHAS, G->num_edges);
+    return hsh;
+}
+
+extern "C" void paradmm_internal_forget_graph(const graph *G)
+{
+    std::lock_guard<std::mutex> lk(g_sweep_mu);
+    auto it = g_cache.find(G);
+    if (it == g_cache.end()) return;
+    for (Cached &c : it->second) paradmm_gpu_destroy(c.h);
+    g_cache.erase(it);
+}
+
+// Handle for G with the requested engine; uploads G's current state.
+static paradmm_gpu *sweep_handle(graph *G, int engine_req)
+{
+    paradmm_gpu_opts o = g_sweep_opts;
+    if (engine_req >= 0) o.engine = engine_req;
+    const uint64_t hh = coef_hash(G);
+    std::vector<Cached> &v = g_cache[G];
+    for (auto it = v.begin(); it != v.end(); ++it) {
+        if (it->engine_req != o.engine) continue;
+        const bool same = it->num_opts == G->num_opts && it->num_vars == G->num_vars && it->num_edges == G->num_edges &&
+                          it->num_dims == G->num_dims && it->ptrs[0] == (const void *)G->operatorix_to_edgelistix &&
+                          it->ptrs[1] == (const void *)G->edgeix_to_varlistix &&
+                          it->ptrs[2] == (const void *)G->list_of_operators_functions_pointers &&
+                          it->ptrs[3] == (const void *)G->varix_to_edgelistix && it->coef_hash == hh;
+        if (same) {
+            if (paradmm_gpu_upload(it->h, G) == PARADMM_OK) return it->h;
+            if (paradmm_last_status() != PARADMM_EUNSUPPORTED_GRAPH) return nullptr;
+        }
+        paradmm_gpu_destroy(it->h);
+        v.erase(it);
+        break;
+    }
+    paradmm_gpu *h = nullptr;
+    if (paradmm_gpu_create(G, &o, &h) != PARADMM_OK) {
+        // a packing-eligible topology whose state cannot be kept compact
+        if (o.engine == PARADMM_ENGINE_AUTO && paradmm_last_status() == PARADMM_EUNSUPPORTED_GRAPH) {
+            o.engine = PARADMM_ENGINE_GENERIC_F64;
+            if (paradmm_gpu_create(G, &o, &h) != PARADMM_OK) return nullptr;
+        } else {
+            return nullptr;
+        }
+    }
+    Cached c;
+    c.h = h;
+    c.engine_req = engine_req >= 0 ? engine_req : g_sweep_opts.engine;
+    c.num_opts = G->num_opts; c.num_vars = G->num_vars; c.num_edges = G->num_edges; c.num_dims = G->num_dims;
+    c.ptrs[0] = G->operatorix_to_edgelistix; c.ptrs[1] = G->edgeix_to_varlistix;
+    c.ptrs[2] = G->list_of_operators_functions_pointers; c.ptrs[3] = G->varix_to_edgelistix;
+    c.coef_hash = hh;
+    v.push_back(c);
+    return h;
+}
+
+// One reference phase (or a whole sweep) on the GPU: upload, run, download.
+static void sweep_call(graph *G, int phase, int iters)
+{
+    std::lock_guard<std::mutex> lk(g_sweep_mu);
+    ok_status();
+    const int engine_req = phase < 0 ? -1 : PARADMM_ENGINE_GENERIC_F64;
+    paradmm_gpu *h = sweep_handle(G, engine_req);
+    if (!h) return;
+    DevGuard guard(h->device);
+    int rc;
+    if (phase < 0) rc = paradmm_gpu_iterate(h, iters);
+    else rc = gen_phase(h, phase);
+    if (rc == PARADMM_OK) rc = paradmm_gpu_download(h, G);
+    (void)rc;
+}
+
+extern "C" void updateXM(graph *G) { sweep_call(G, GEN_PHASE_XM, 1); }
+extern "C" void updateX(graph *G) { sweep_call(G, GEN_PHASE_X, 1); }
+extern "C" void updateM(graph *G) { sweep_call(G, GEN_PHASE_M, 1); }
+extern "C" void updateZ(graph *G) { sweep_call(G, GEN_PHASE_Z, 1); }
+extern "C" void updateUN(graph *G) { sweep_call(G, GEN_PHASE_UN, 1); }
+extern "C" void updateU(graph *G) { sweep_call(G, GEN_PHASE_U, 1); }
+extern "C" void updateN(graph *G) { sweep_call(G, GEN_PHASE_N, 1); }
+extern "C" void updateG(graph *G) { sweep_call(G, -1, 1); }
+extern "C" void update_outgoing_rhos(graph *G) { (void)G; }  // a no-op in the reference too (core/paradmm.c:564-566)
+extern "C" void updateXOpenMP(graph *G) { updateX(G); }
+extern "C" void updateMOpenMP(graph *G) { updateM(G); }
+extern "C" void updateZOpenMP(graph *G) { updateZ(G); }
+extern "C" void updateUOpenMP(graph *G) { updateU(G); }
+extern "C" void updateNOpenMP(graph *G) { updateN(G); }
+extern "C" void updateGOpenMP(graph *G, int maxiter, int numthreads)
+{
+    (void)numthreads;
+    if (maxiter <= 0) return;
+    sweep_call(G, -1, maxiter);
+}

@@ -1,0 +1,86 @@
+// Host-side internals of the engine shared by engine.cu and the drop-in
+// sweep functions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "generic.cuh"
+#include "packing.cuh"
+
+int pdm_set_error(int status, const char *fmt, ...);
+
+// Result of classifying a host graph.
+struct GraphInfo {
+    int ok = 0;                    // all factors known and well-formed
+    std::vector<int> kind;         // per factor PARADMM_OP_*
+    // packing structure (valid when packing_ok)
+    int packing_ok = 0;
+    std::string packing_why;       // why the packing engine cannot run it
+    int N = 0;                     // circles
+    std::vector<int> centre_var, radius_var;  // per circle
+    std::vector<int> circle_of_var;           // -1 if none
+};
+
+struct PkHost {
+    int V = 2, BW = 64;
+    bool stream_hint = true;
+    int dynamic = 1;
+    int grid = 0;
+    int n_inst = 0, n_items = 0, n_circ = 0;
+    long long n_tiles = 0;
+    int n_wall = 0, n_rad = 0;
+    std::vector<PkInst> inst;
+    std::vector<int4> items;
+    std::vector<PkCircle> circ;
+    std::vector<float4> wall_vp, wall_coef;
+    std::vector<double2> wall_rho;
+    std::vector<int> wall_circle;   // local circle of each wall (within its instance)
+    std::vector<float4> rad_coef;
+    std::vector<double> rad_rho;
+    std::vector<int> rad_circle;
+    std::vector<int> wall_base, rad_base;  // per instance
+    std::vector<double> init_Z;      // per global circle (cx, cy, r)
+    PkDev D{};
+    long long it_next = 0;           // global sweep counter
+    std::vector<long long> upload_iter;
+    std::vector<int> nmode;
+    std::vector<PkStatus> status;    // host copy after the last launch
+    std::vector<long long> iters_last_call;
+    // reference-layout maps (graph handles)
+    int2 *d_pmap = nullptr; long long n_pmap = 0;
+    int *d_wmap = nullptr, *d_rmap = nullptr, *d_wcirc = nullptr, *d_rcirc = nullptr;
+    int2 *d_cmap = nullptr;
+    int *d_flag = nullptr;
+    unsigned long long *d_viol = nullptr;
+};
+
+struct GenHost {
+    GenDev D{};
+    std::vector<int> radius_vars;    // for the total-radius metric
+    double *d_Zprev = nullptr;
+    double *d_acc = nullptr;         // residual sums
+    unsigned long long *d_viol = nullptr;
+    int zprev_valid = 0;
+    double last_primal = -1, last_dual = -1;
+};
+
+struct paradmm_gpu {
+    int engine = PARADMM_ENGINE_AUTO;
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    paradmm_gpu_opts opts{};
+    int from_graph = 0;
+    int num_dims = 0, num_vars = 0, num_edges = 0, num_opts = 0;
+    GenHost *gen = nullptr;
+    PkHost *pk = nullptr;
+    DevCtl *ctl = nullptr;
+    double *d_stage[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // X M N U Z in reference layout
+    std::vector<void *> allocs;
+    long long device_bytes = 0;
+};

@@ -1,0 +1,127 @@
+// Fused circle-packing ADMM engine: data layout shared by kernels and host.
+//
+// Problem (per instance): N circles; circle i owns the centre variable c_i
+// (2 components) and the radius variable r_i (2 components in the reference,
+// both always equal here, so one is stored).  Factors:
+//   pair   (i < j): edges [c_i, r_i, c_j, r_j]  disk_collision_variable_radius
+//                   (packing/host.c:83-132)
+//   wall   (i, w):  edges [c_i, r_i]            disk_plane_collision_variable_radius
+//                   (packing/host.c:31-65)
+//   radius (i):     edge  [r_i]                 maximize_sum_of_squared_disk_radii_alpha
+//                   (packing/host.c:10-29, 67-81)
+//
+// One ADMM sweep (reference core/paradmm.c:736-741: updateXM, updateZ,
+// updateUN) is restated as ONE pass over the edge state plus a consensus
+// finalisation.  The state kept per live edge component is X^k and U^(k-1)
+// (FP32); sweep k+1 then does, per component,
+//     U^k = U^(k-1) + alpha (X^k - Z^k)      (updateU of sweep k)
+//     N^k = Z^k - U^k                        (updateN of sweep k)
+//     X^(k+1) = prox(N^k)                    (updateX of sweep k+1)
+//     M = X^(k+1) + U^k                      (updateM of sweep k+1)
+// and accumulates rho*M into per-circle FP64 partial sums, which the
+// finalisation turns into Z^(k+1) (updateZ of sweep k+1).  So each sweep
+// reads and writes X and U once: 16 bytes per live component.
+//
+// Pair state layout.  Circles are cut into blocks of BW = 32*V; the pairs of
+// block I against block J >= I form tile (I, J), numbered row-major over the
+// upper triangle.  A tile is BW rows (circle i) x 6 components x BW columns
+// (circle j) x {X, U} floats:
+//     tile[row][comp][col][xu],   comp = cx_i, cy_i, r_i, cx_j, cy_j, r_j
+// so the 32 lanes of a warp, lane l owning columns [V l, V l + V), read and
+// write one row's component as one contiguous 256*V-byte segment (V = 2:
+// one float4 per lane holding X,U of two columns).  Diagonal tiles only use
+// col > row; slots outside the triangle or past N are never touched.
+#pragma once
+
+#include <stdint.h>
+
+#include "common.cuh"
+
+#define PK_THREADS 256
+#define PK_WARPS (PK_THREADS / 32)
+#define PK_COMPS 6
+
+// Per-instance constants.
+struct PkInst {
+    int N;                  // circles
+    int nb;                 // circle blocks (ceil(N / BW))
+    int circle_base;        // global index of the instance's circle 0
+    int item_base;          // first work item
+    int n_items;            // work items (pair tiles + circle blocks)
+    int pad0;
+    long long tile_base;    // global index of tile (0, 0)
+    float alpha[4];         // pair edge steps by position (c_i, r_i, c_j, r_j)
+    float A1, A2, B2m1, C1; // pair prox coefficients (see pair_prox)
+    float D1, C2, D2, pad1;
+    double rho[4];          // pair edge penalties by position (FP64, consensus weights)
+    double inv_ncomp;       // 1 / (num_edges * num_dims) of the reference graph
+    double pad2;
+};
+
+// Per-circle constants (global circle index).
+struct PkCircle {
+    double inv_rho_c;   // 1 / sum of rho over the centre variable's edges
+    double inv_rho_r;   // 1 / sum of rho over the radius variable's edges
+    double w_c;         // edges of the centre variable (dual-residual weight per dim)
+    double w_r;         // 2 x edges of the radius variable (both dims)
+    int wall_start, wall_count;
+    int rad_start, rad_count;
+    int inst;
+    int pad[3];
+};
+
+// Work item: x = instance, y = kind (0 pair tile, 1 circle block),
+// kind 0: z = I, w = J (block indices); kind 1: z = first circle, w = count.
+// (int4)
+
+// Per-instance run status, written by the kernel.
+struct PkStatus {
+    long long last_iter;    // last sweep index this instance executes (LLONG_MAX: none yet)
+    long long check_from;   // first sweep index whose finalisation may stop it
+    long long resid_iter;   // iterate the residuals below belong to (-1: none)
+    double primal, dual;
+    int converged;
+    int nonfinite;
+    int nmode;              // X slots hold N (state uploaded from a graph) for the first sweep
+    int pad;
+};
+
+// Device pointers of a packing handle (passed by value to kernels).
+struct PkDev {
+    const PkInst *inst;
+    const int4 *items;
+    const PkCircle *circ;
+    const int *claim;        // [n_items] order in which blocks claim items (largest first)
+    int n_inst, n_items, n_circ, pad;
+    float *tiles;            // pair state
+    double4 *row_part;       // [tile][BW] sums of M over the row circle's pair edges
+    double4 *col_part;       // [tile][BW] same for the column circle
+    double4 *Z;              // [circle] consensus (cx, cy, r, -)
+    double4 *local_part;     // [circle] rho-weighted wall + radius contributions
+    double *circ_dual;       // [2][n_circ] dual-residual partials by parity
+    double *item_primal;     // [2][n_items] primal-residual partials by parity
+    PkStatus *status;        // [n_inst]
+    // walls (sorted by circle)
+    const float4 *wall_vp;   // v_x, v_y, p_x, p_y
+    const float4 *wall_coef; // rho_c, rho_r, alpha_c, alpha_r
+    const double2 *wall_rho; // rho_c, rho_r (FP64)
+    float4 *wall_X;          // cx, cy, r, -
+    float4 *wall_U;
+    // radius factors (sorted by circle)
+    const float4 *rad_coef;  // exponent, rho, alpha, -
+    const double *rad_rho;
+    float2 *rad_XU;          // X, U of the radius edge
+    struct DevCtl *ctl;
+};
+
+struct PkRun {
+    long long it0;    // global sweep index of the launch's first sweep
+    int n_iter;       // sweeps to run
+    int dynamic;      // dynamic work-item scheduling
+    double tol;       // stop when primal + dual <= tol (tol < 0: never)
+    int check_every;  // sweeps between stopping checks
+    int pad;
+};
+
+PDM_HD long long pk_tri(int I, int J, int nb) { return (long long)I * nb - (long long)I * (I - 1) / 2 + (J - I); }
+PDM_HD long long pk_tile_floats(int BW) { return (long long)BW * PK_COMPS * 2 * BW; }

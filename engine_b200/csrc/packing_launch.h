@@ -1,0 +1,18 @@
+// Host-side launchers of the packing kernels (packing_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "packing.cuh"
+
+cudaError_t pk_launch_persistent(int V, bool stream_hint, const PkDev &D, const PkRun &R, int grid, cudaStream_t s);
+cudaError_t pk_max_blocks_per_sm(int V, bool stream_hint, int *blocks);
+cudaError_t pk_launch_init(int V, const PkDev &D, int inst, const float *pair_duals, int grid, cudaStream_t s);
+cudaError_t pk_launch_scatter(int V, const PkDev &D, int inst, const int2 *pmap, long long npairs, const int *wmap,
+                              int wall0, int nwall, const int *rmap, int rad0, int nrad, const int2 *cmap,
+                              const double *Nd, const double *Ud, const double *Zd, int *flag, int grid, cudaStream_t s);
+cudaError_t pk_launch_gather(int V, const PkDev &D, int inst, const int2 *pmap, long long npairs, const int *wmap,
+                             int wall0, int nwall, const int *rmap, int rad0, int nrad, const int2 *cmap,
+                             const int *wcirc, const int *rcirc, int nmode, double *Xo, double *Mo, double *No,
+                             double *Uo, double *Zo, int grid, cudaStream_t s);
+cudaError_t pk_launch_violation(const PkDev &D, unsigned long long *out, int grid, cudaStream_t s);

@@ -1,0 +1,195 @@
+/*
+ * paradmm_gpu.h -- C-ABI of the B200 parADMM engine (libparadmm_b200.so).
+ *
+ * Replaces the reference GPU back-end (core/paradmm-gpu.h:16-29 and the
+ * user-launched kernel loop of packing/gpu.cu:257-291): instead of deep
+ * copying the graph with one cudaMalloc per factor and launching five kernels
+ * per sweep, a caller creates an engine handle from a host `graph`
+ * (paradmm.h), iterates or solves on the device, and downloads the state back
+ * into the graph in the reference's FP64 [edge][dim] layout.
+ *
+ * Every function returns PARADMM_OK (0) or a negative PARADMM_E* code and
+ * never exits the process; paradmm_last_error_string() describes the last
+ * failure of the calling thread.  A handle owns its device memory and its
+ * CUDA stream; calls on one handle are synchronous and must not overlap.
+ *
+ * Engines.  A graph whose factors are the three circle-packing operators
+ * (pair non-overlap, half-plane wall, radius reward) over consistent
+ * (centre, radius) variable couples, with every pair of circles present once
+ * and per-position uniform pair penalties, runs on the fused packing engine:
+ * FP32 edge state in a tiled structure-of-arrays layout, FP64 consensus and
+ * residuals, one persistent grid-synchronised kernel for many sweeps.  Any
+ * other graph of those operators runs on the generic engine (CSR incidence,
+ * FP64 or FP32 state, reference summation order).  Graphs with operators the
+ * engine does not know are rejected with PARADMM_EUNSUPPORTED_OP.
+ */
+#ifndef PARADMM_B200_PARADMM_GPU_H
+#define PARADMM_B200_PARADMM_GPU_H
+
+#include <stdint.h>
+#include "paradmm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+enum {
+    PARADMM_OK = 0,
+    PARADMM_EINVAL = -1,             /* bad argument or inconsistent graph        */
+    PARADMM_ENOMEM = -2,             /* host or device allocation failed          */
+    PARADMM_ECUDA = -3,              /* CUDA runtime error                        */
+    PARADMM_EUNSUPPORTED_OP = -4,    /* a factor's operator is not known          */
+    PARADMM_EUNSUPPORTED_GRAPH = -5, /* the requested engine cannot run this graph */
+    PARADMM_ENONFINITE = -6,         /* NaN/Inf appeared in the residuals         */
+    PARADMM_ETIMEOUT = -7,           /* a device-side wait ran out (grid barrier) */
+    PARADMM_ENODEVICE = -8           /* no usable CUDA device                     */
+};
+
+/* ---- operator kinds (the three packing operators, packing/host.c:31-132) ---- */
+enum {
+    PARADMM_OP_UNKNOWN = 0,
+    PARADMM_OP_PAIR = 1,   /* disk_collision_variable_radius, 4 edges          */
+    PARADMM_OP_WALL = 2,   /* disk_plane_collision_variable_radius, 2 edges,
+                              params = [v (numdims), p (numdims)] doubles     */
+    PARADMM_OP_RADIUS = 3  /* maximize_sum_of_squared_disk_radii_alpha, any
+                              number of edges, params[0] = exponent           */
+};
+
+/* ---- engine selection ---- */
+enum {
+    PARADMM_ENGINE_AUTO = 0,        /* packing engine when eligible, else generic FP64 */
+    PARADMM_ENGINE_PACKING = 1,     /* fused packing engine (FP32 state, FP64 consensus) */
+    PARADMM_ENGINE_GENERIC_F64 = 2, /* CSR engine, FP64, reference summation order       */
+    PARADMM_ENGINE_GENERIC_F32 = 3  /* CSR engine, FP32 state, FP64 consensus            */
+};
+
+typedef struct paradmm_gpu paradmm_gpu; /* opaque engine handle */
+
+typedef struct paradmm_gpu_opts {
+    int device;       /* CUDA device ordinal                                   */
+    int engine;       /* PARADMM_ENGINE_*                                      */
+    int block_width;  /* packing engine: circles per tile side (32, 64, 128); 0 = tuned */
+    int ctas_per_sm;  /* packing engine: resident CTAs per SM; 0 = tuned       */
+    int check_every;  /* sweeps between residual-based stopping checks; 0 = 1  */
+    int reserved[8];
+} paradmm_gpu_opts;
+
+typedef struct paradmm_stats {
+    int64_t iterations;   /* sweeps performed by the call                       */
+    int converged;        /* 1 when primal + dual <= tol was met                */
+    int status;           /* PARADMM_OK or the error that stopped the call      */
+    double primal;        /* RMS over all (edge, dim) of X - Z_v(e)             */
+    double dual;          /* RMS over all (edge, dim) of Z_v(e) - Zprev_v(e)    */
+    double max_violation; /* packing: max pair overlap / wall penetration / -r  */
+    double total_radius;  /* packing: sum of consensus radii                    */
+    double device_ms;     /* device time of the call                            */
+} paradmm_stats;
+
+/* Default options (device 0, AUTO engine, tuned shapes). */
+void paradmm_gpu_default_opts(paradmm_gpu_opts *opts);
+
+/* Declares that host function `op` is one of the packing operators, so that
+ * graphs built with the caller's own copy of that operator are accepted.
+ * The library's exported operators (paradmm.h) are known without this. */
+int paradmm_gpu_register_op(paradmm_op_fn op, int kind);
+
+/* Builds a handle for graph G: classifies its factors, lays out the state on
+ * the device and uploads the state arrays (X, N, U, Z, RHOS, ALPHAS) that G
+ * holds.  G is only read; the handle does not keep pointers into it. */
+int paradmm_gpu_create(const graph *G, const paradmm_gpu_opts *opts, paradmm_gpu **out);
+
+/* Re-uploads the state arrays of G (same topology as at create). */
+int paradmm_gpu_upload(paradmm_gpu *h, const graph *G);
+
+/* Runs n full sweeps (updateG semantics). */
+int paradmm_gpu_iterate(paradmm_gpu *h, int n);
+
+/* Runs up to maxiter sweeps, stopping once primal + dual <= tol (tol <= 0:
+ * never).  The check lags one sweep: the state returned is one sweep past the
+ * first iterate whose residuals met the tolerance.  stats may be NULL. */
+int paradmm_gpu_solve(paradmm_gpu *h, int maxiter, double tol, paradmm_stats *stats);
+
+/* Writes X, M, N, U and Z of the current iterate into G (reference layout,
+ * FP64).  G must have the create-time topology and allocated state arrays. */
+int paradmm_gpu_download(paradmm_gpu *h, graph *G);
+
+/* Residuals and packing metrics of the current iterate. */
+int paradmm_gpu_stats(paradmm_gpu *h, paradmm_stats *out);
+
+/* Which engine the handle runs (PARADMM_ENGINE_*). */
+int paradmm_gpu_engine(const paradmm_gpu *h);
+
+void paradmm_gpu_destroy(paradmm_gpu *h);
+
+/* ---- structured packing problems (no host graph needed) ----
+ *
+ * Describes the graph the reference demo builds (packing/host.c:283-343):
+ * n_circles circles, one radius factor per circle, each listed half-plane
+ * applied to every circle, and every pair of circles, with penalties rho
+ * (rho_radius on the radius factors' edges) and step alpha.  Initial state:
+ * Z from `init` ([cx, cy, r] per circle), X_e = Z_v(e), U = 0.  Its edge
+ * numbering is that of the graph built in packing/host.c's order: radius
+ * factors, then walls (wall-major), then pairs (row-major i < j). */
+typedef struct paradmm_packing_desc {
+    int n_circles;
+    int n_walls;          /* <= 8 */
+    const double *walls;  /* n_walls x [v_x, v_y, p_x, p_y]: v.(c - p) + r <= 0 */
+    double exponent;      /* radius reward exponent (params[0] of the radius op) */
+    double rho;           /* penalty of pair and wall edges                     */
+    double rho_radius;    /* penalty of radius-factor edges                     */
+    double alpha;         /* dual step on every edge                            */
+    const double *init;   /* n_circles x [cx, cy, r]                            */
+} paradmm_packing_desc;
+
+/* One handle holding `count` independent packing instances (count = 1 for a
+ * single problem).  Instances may differ in every field.  They share one
+ * persistent launch; each stops on its own residual in solve. */
+int paradmm_gpu_create_packing(const paradmm_packing_desc *descs, int count,
+                               const paradmm_gpu_opts *opts, paradmm_gpu **out);
+
+/* Number of instances of a handle (1 for graph handles). */
+int paradmm_gpu_instances(const paradmm_gpu *h);
+
+/* Per-instance statistics of the last solve / current state
+ * (stats must hold paradmm_gpu_instances(h) entries). */
+int paradmm_gpu_instance_stats(paradmm_gpu *h, paradmm_stats *stats);
+
+/* Consensus circles [cx, cy, r] of one instance (n_circles x 3 doubles). */
+int paradmm_gpu_get_circles(paradmm_gpu *h, int instance, double *out);
+
+/* Replaces an instance's state by a warm start: consensus Z from `circles`
+ * ([cx, cy, r] per circle), X_e = Z_v(e), and the duals U of the pair edges
+ * from `pair_duals` (may be NULL for U = 0).  pair_duals holds, for every
+ * pair i < j in row-major order, the six pair-edge duals
+ * [u_cx_i, u_cy_i, u_r_i, u_cx_j, u_cy_j, u_r_j]. */
+int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double *circles, const float *pair_duals);
+
+/* Device memory the handle holds, in bytes. */
+int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h);
+
+/* Appends the factors of the reference demo's packing graph to G (which
+ * must be fresh from startG(G, 2)): one radius factor per circle on var 2i+1,
+ * each of the n_walls half-planes on every circle (vars 2i, 2i+1), and every
+ * pair i < j (vars 2i, 2i+1, 2j, 2j+1), by addNode, in packing/host.c's order
+ * (order = 0: radius, walls, pairs) or packing/gpu.cu's (order = 1: walls,
+ * radius, pairs).  walls (n_walls x 4 doubles) and exponent (1 double) are
+ * borrowed by the graph like any addNode parameter and must outlive it.
+ * A fast bulk replacement for the reference demo's construction loops
+ * (packing/host.c:299-335). */
+int paradmm_add_packing_factors(graph *G, int n_circles, int n_walls, double *walls, double *exponent, int order);
+
+/* ---- errors ---- */
+int paradmm_last_status(void);
+const char *paradmm_last_error_string(void);
+
+/* ---- engine used by the paradmm.h sweep functions (updateG, ...) ----
+ * The drop-in sweep functions build (and cache, per graph pointer, until
+ * closeG) a handle with these options. */
+void paradmm_set_sweep_options(const paradmm_gpu_opts *opts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARADMM_B200_PARADMM_GPU_H */

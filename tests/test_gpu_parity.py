@@ -1,0 +1,240 @@
+"""GPU parity: the engine against the reference's own CPU path.
+
+The oracle is the reference C (core/paradmm.c + packing/host.c) compiled
+from its own sources into oracle/_ref (or, without it, the C restatement
+oracle/paradmm_port.c, which tests/test_oracle.py pins bit-for-bit to it).
+
+Tolerances:
+  generic engine, FP64   bit-identical (reference summation order, no FMA)
+  packing engine, FP32   max |difference| <= 1e-4 per iterate (north star:
+                         FP32 edge state, per-iterate max abs diff 1e-4)
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import engine_b200 as eb
+import oracle_lib
+
+pytestmark = pytest.mark.gpu
+
+TOL_F32 = 1e-4
+RHO, RHO_R, ALPHA, EXP = 10.0, 5.0, 1.0, 2.0
+
+
+def problem(N, seed, W=1.0, H=1.0, rmax=0.05, order=0, lib=None):
+    walls = eb.box_walls(W, H)
+    circles = eb.seeded_circles(N, W, H, rmax, seed)
+    pg = eb.PackingGraph(N, walls, EXP, order=order)
+    pg.init_seeded(circles, RHO, RHO_R, ALPHA)
+    orc = oracle_lib.OraclePacking(lib or oracle_lib.best(), N, walls, EXP, order=order)
+    orc.init(seed, W, H, rmax, RHO, RHO_R, ALPHA)
+    return pg, orc, circles
+
+
+def maxdiff(a: dict, b: dict) -> float:
+    return max(float(np.max(np.abs(a[k] - b[k]))) for k in ("X", "M", "N", "U", "Z"))
+
+
+def assert_same(a: dict, b: dict):
+    for k in ("X", "M", "N", "U", "Z"):
+        assert np.array_equal(a[k], b[k]), f"{k} differs (max {np.max(np.abs(a[k] - b[k]))})"
+
+
+# ------------------------------------------------------------ generic FP64
+@pytest.mark.parametrize("order", [0, 1])
+def test_generic_f64_bit_identical_to_reference(order):
+    pg, orc, _ = problem(24, 11, order=order)
+    assert_same(pg.G.state(), orc.state())
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_GENERIC_F64) as h:
+        assert h.engine() == eb.ENGINE_GENERIC_F64
+        h.iterate(300)
+        h.download(pg.G)
+    orc.run(300, trace=False)
+    assert_same(pg.G.state(), orc.state())
+
+
+def test_generic_f64_random_full_state():
+    """Reference-style random state (both radius dims differ): all dims evolve."""
+    pg, orc, _ = problem(16, 5)
+    rng = np.random.default_rng(3)
+    st = {k: rng.uniform(-1, 2, size=v.shape) for k, v in orc.state().items()}
+    orc.set_state(st)
+    for k, v in st.items():
+        pg.G.arr(k)[:] = v
+    with eb.Handle.from_graph(pg.G) as h:  # AUTO must fall back to the generic engine
+        assert h.engine() == eb.ENGINE_GENERIC_F64
+        h.iterate(40)
+        h.download(pg.G)
+    orc.run(40, trace=False)
+    assert_same(pg.G.state(), orc.state())
+
+
+@pytest.mark.parametrize("phase", ["updateX", "updateM", "updateXM", "updateZ", "updateU", "updateN", "updateUN",
+                                   "updateG"])
+def test_dropin_phase_functions_bit_identical(phase):
+    pg, orc, _ = problem(12, 7)
+    rng = np.random.default_rng(9)
+    st = {k: rng.uniform(0, 1, size=v.shape) for k, v in orc.state().items()}
+    orc.set_state(st)
+    for k, v in st.items():
+        pg.G.arr(k)[:] = v
+    lib = eb.load()
+    o = eb.opts(engine=eb.ENGINE_GENERIC_F64)
+    lib.paradmm_set_sweep_options(C.byref(o))
+    try:
+        getattr(lib, phase)(C.byref(pg.G))
+        assert eb.last_status() == eb.OK, eb.last_error()
+    finally:
+        lib.paradmm_set_sweep_options(None)
+    getattr(orc.lib, phase)(orc.graph_ptr())
+    assert_same(pg.G.state(), orc.state())
+
+
+def test_dropin_updateGOpenMP_generic():
+    pg, orc, _ = problem(20, 8)
+    lib = eb.load()
+    o = eb.opts(engine=eb.ENGINE_GENERIC_F64)
+    lib.paradmm_set_sweep_options(C.byref(o))
+    try:
+        lib.updateGOpenMP(C.byref(pg.G), 25, 8)
+        assert eb.last_status() == eb.OK, eb.last_error()
+    finally:
+        lib.paradmm_set_sweep_options(None)
+    orc.run(25, trace=False)
+    assert_same(pg.G.state(), orc.state())
+
+
+# ---------------------------------------------------------- packing FP32
+@pytest.mark.parametrize("bw", [32, 64, 128])
+def test_packing_teacher_forced_one_sweep(bw):
+    """From oracle iterate k, one engine sweep vs oracle iterate k+1."""
+    N = 150
+    pg, orc, _ = problem(N, 21)
+    worst = 0.0
+    done = 0
+    for k in (0, 1, 5, 40, 200, 600):
+        orc.run(k - done, trace=False)
+        done = k
+        st = orc.state()
+        for key, v in st.items():
+            pg.G.arr(key)[:] = v
+        with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING, block_width=bw) as h:
+            h.iterate(1)
+            h.download(pg.G)
+        orc.sweep()
+        done += 1
+        d = maxdiff(pg.G.state(), orc.state())
+        worst = max(worst, d)
+        assert d <= TOL_F32, f"k={k}: max diff {d}"
+    print(f"teacher-forced worst max|diff| = {worst:.3e}")
+
+
+def test_packing_free_running_20():
+    N = 120
+    pg, orc, _ = problem(N, 4)
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
+        for k in range(20):
+            h.iterate(1)
+            h.download(pg.G)
+            orc.sweep()
+            d = maxdiff(pg.G.state(), orc.state())
+            assert d <= TOL_F32, f"iterate {k + 1}: max diff {d}"
+
+
+def test_dropin_updateG_runs_packing_engine():
+    pg, orc, _ = problem(40, 2)
+    lib = eb.load()
+    lib.paradmm_set_sweep_options(None)
+    for _ in range(5):
+        lib.updateG(C.byref(pg.G))
+        assert eb.last_status() == eb.OK, eb.last_error()
+        orc.sweep()
+    assert maxdiff(pg.G.state(), orc.state()) <= TOL_F32
+    lib.updateGOpenMP(C.byref(pg.G), 30, 8)
+    orc.run(30, trace=False)
+    assert maxdiff(pg.G.state(), orc.state()) <= 1e-3  # 35 free-running FP32 sweeps
+    lib.closeG(C.byref(pg.G))
+
+
+def test_upload_download_roundtrip_without_sweep():
+    pg, orc, _ = problem(30, 9)
+    orc.run(7, trace=False)
+    st = orc.state()
+    for k, v in st.items():
+        pg.G.arr(k)[:] = v
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
+        for k in ("N", "U", "Z"):
+            pg.G.arr(k)[:] = 0.0
+        h.download(pg.G)
+    got = pg.G.state()
+    for k in ("N", "U", "Z"):
+        assert np.max(np.abs(got[k] - st[k])) <= 1e-6 * max(1.0, np.max(np.abs(st[k])))
+
+
+def test_structured_handle_matches_graph_handle():
+    N = 90
+    pg, orc, circles = problem(N, 13)
+    desc = dict(n_circles=N, walls=eb.box_walls(1, 1), exponent=EXP, rho=RHO, rho_radius=RHO_R, alpha=ALPHA,
+                init=circles)
+    with eb.Handle.packing([desc], block_width=64) as hs, \
+            eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING, block_width=64) as hg:
+        hs.iterate(100)
+        hg.iterate(100)
+        hg.download(pg.G)
+        a = hs.circles(0, N)
+    Z = pg.G.arr("Z")
+    b = np.stack([Z[0::2, 0], Z[0::2, 1], Z[1::2, 0]], axis=1)
+    assert np.max(np.abs(a - b)) <= 1e-5
+
+
+def test_batched_equals_single_instances():
+    rng = np.random.default_rng(0)
+    descs = []
+    for i in range(6):
+        N = int(rng.integers(20, 150))
+        asp = float(rng.uniform(1, 2))
+        descs.append(dict(n_circles=N, walls=eb.box_walls(asp, 1.0), exponent=EXP, rho=RHO, rho_radius=RHO_R,
+                          alpha=ALPHA, init=eb.seeded_circles(N, asp, 1.0, 0.05, 100 + i)))
+    with eb.Handle.packing(descs, block_width=64) as hb:
+        hb.iterate(150)
+        batched = [hb.circles(i, d["n_circles"]) for i, d in enumerate(descs)]
+    for i, d in enumerate(descs):
+        with eb.Handle.packing([d], block_width=64) as h1:
+            h1.iterate(150)
+            single = h1.circles(0, d["n_circles"])
+        assert np.array_equal(batched[i], single), f"instance {i} differs"
+
+
+def test_solve_reaches_tolerance_and_metrics():
+    N = 50
+    pg, orc, circles = problem(N, 31)
+    desc = dict(n_circles=N, walls=eb.box_walls(1, 1), exponent=EXP, rho=RHO, rho_radius=RHO_R, alpha=ALPHA,
+                init=circles)
+    with eb.Handle.packing([desc]) as h:
+        s = h.solve(40000, 1e-5)
+        st = h.instance_stats()[0]
+    assert s["converged"] == 1, s
+    assert st["primal"] + st["dual"] <= 1e-5
+    n, tr = orc.run(40000, tol=1e-5)
+    m = tr[-1]
+    print(f"engine FP32: iters {s['iterations']} r {st['primal']:.2e} s {st['dual']:.2e} "
+          f"viol {st['max_violation']:.2e} total radius {st['total_radius']:.6f}")
+    print(f"oracle FP64: iters {n} r {m[0]:.2e} s {m[1]:.2e} viol {m[2]:.2e} total radius {m[3]:.6f}")
+    assert st["max_violation"] < 5e-3
+    assert abs(st["total_radius"] - m[3]) / m[3] < 0.1
+
+
+def test_nonfinite_is_reported():
+    """Two coincident centres make the pair operator divide 0/0 (as the
+    reference does, packing/host.c:123): the engine stops with ENONFINITE."""
+    N = 10
+    circles = eb.seeded_circles(N, 1, 1, 0.3, 1)
+    circles[1, :2] = circles[0, :2]
+    desc = dict(n_circles=N, walls=eb.box_walls(1, 1), exponent=EXP, rho=RHO, rho_radius=RHO_R, alpha=ALPHA,
+                init=circles)
+    with eb.Handle.packing([desc]) as h:
+        s = h.solve(50, -1.0)
+        assert s["status"] == eb.ENONFINITE
+        assert eb.last_status() == eb.ENONFINITE
