@@ -138,6 +138,11 @@ _SIGS = {
     "paradmm_gpu_get_circles": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "paradmm_gpu_warm_start": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     "paradmm_gpu_device_bytes": (C.c_int64, [C.c_void_p]),
+    "paradmm_gpu_launches": (C.c_int64, [C.c_void_p]),
+    "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "paradmm_gpu_pin_graph": (C.c_int, [C.POINTER(Graph)]),
+    "paradmm_gpu_unpin_graph": (C.c_int, [C.POINTER(Graph)]),
     "paradmm_last_status": (C.c_int, []),
     "paradmm_last_error_string": (C.c_char_p, []),
     "paradmm_set_sweep_options": (None, [C.POINTER(Opts)]),
@@ -392,6 +397,18 @@ class Handle:
 
     def device_bytes(self) -> int:
         return self.lib.paradmm_gpu_device_bytes(self.ptr)
+
+    def launches(self) -> int:
+        return self.lib.paradmm_gpu_launches(self.ptr)
+
+    def set_profiling(self, on: bool) -> None:
+        check(self.lib.paradmm_gpu_set_profiling(self.ptr, 1 if on else 0))
+
+    def phase_times(self) -> list[float]:
+        """Mean block time per sweep (us): pass, barrier 1, finalise, barrier 2."""
+        out = (C.c_double * 4)()
+        check(self.lib.paradmm_gpu_phase_times(self.ptr, out))
+        return list(out)
 
     def close(self) -> None:
         if self.ptr and self.ptr.value:

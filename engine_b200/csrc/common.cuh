@@ -26,7 +26,8 @@ struct DevCtl {
     int err;                  // DEV_* error, first writer wins
     int n_active;             // instances still iterating
     unsigned int item_ctr[2]; // dynamic work counters, one per iteration parity
-    unsigned int pad[2];
+    unsigned int pad[2];      // pad[0]: sweeps completed by the launch
+    unsigned long long prof[4];  // optional: summed block time in pass, barrier 1, finalise, barrier 2 (ns)
 };
 
 // Barrier waits give up after this long; the kernel then records

@@ -12,6 +12,7 @@
 #include <climits>
 #include <cmath>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -724,9 +725,11 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
         R.dynamic = P.dynamic;
         R.tol = tol;
         R.check_every = check_every < 1 ? 1 : check_every;
+        R.prof = P.prof;
         PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
         cudaError_t e = pk_launch_persistent(P.V, P.stream_hint, P.D, R, P.grid, h->stream);
         if (e != cudaSuccess) return pdm_cuda_fail(e, "packing persistent launch", __FILE__, __LINE__);
+        ++h->launches;
         PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
         PDM_CUDA(cudaMemcpyAsync(&c, h->ctl, sizeof c, cudaMemcpyDeviceToHost, h->stream));
         PDM_CUDA(cudaMemcpyAsync(st.data(), P.D.status, sizeof(PkStatus) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
@@ -737,6 +740,8 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
         if (c.err != DEV_OK)
             return pdm_set_error(PARADMM_ETIMEOUT, "packing kernel: a grid barrier wait ran out (device error %d)", c.err);
         const long long sweeps = (long long)c.pad[0];
+        if (P.prof && sweeps > 0)
+            for (int q = 0; q < 4; ++q) P.phase_us[q] = (double)c.prof[q] / 1e3 / P.grid / (double)sweeps;
         for (int i = 0; i < P.n_inst; ++i) {
             if (done[i]) continue;
             const long long last = std::min(st[i].last_iter, it0 + sweeps - 1);
@@ -861,6 +866,7 @@ static int gen_phase(paradmm_gpu *h, int phase)
 {
     cudaError_t e = gen_launch_phase(h->gen->D, phase, h->stream);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "generic phase kernel", __FILE__, __LINE__);
+    ++h->launches;
     return PARADMM_OK;
 }
 
@@ -1109,6 +1115,60 @@ extern "C" int paradmm_gpu_stats(paradmm_gpu *h, paradmm_stats *out)
 extern "C" int paradmm_gpu_engine(const paradmm_gpu *h) { return h ? h->engine : PARADMM_EINVAL; }
 extern "C" int paradmm_gpu_instances(const paradmm_gpu *h) { return !h ? 0 : (h->pk ? h->pk->n_inst : 1); }
 extern "C" int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h) { return h ? h->device_bytes : 0; }
+extern "C" int64_t paradmm_gpu_launches(const paradmm_gpu *h) { return h ? h->launches : 0; }
+
+extern "C" int paradmm_gpu_set_profiling(paradmm_gpu *h, int on)
+{
+    ok_status();
+    if (!h || !h->pk) return pdm_set_error(PARADMM_EINVAL, "profiling needs a packing handle");
+    h->pk->prof = on ? 1 : 0;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_phase_times(const paradmm_gpu *h, double out[4])
+{
+    ok_status();
+    if (!h || !h->pk || !out) return pdm_set_error(PARADMM_EINVAL, "profiling needs a packing handle");
+    for (int q = 0; q < 4; ++q) out[q] = h->pk->phase_us[q];
+    return PARADMM_OK;
+}
+
+// ---- pinned host state (large graphs move through pinned pages) ----
+static std::mutex g_pin_mu;
+static std::unordered_map<const graph *, std::vector<void *>> g_pinned;
+
+extern "C" int paradmm_gpu_pin_graph(const graph *G)
+{
+    ok_status();
+    if (!G || !G->X || !G->M || !G->N || !G->U || !G->Z) return pdm_set_error(PARADMM_EINVAL, "graph state is not allocated");
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (g_pinned.count(G)) return PARADMM_OK;
+    const size_t ne = (size_t)G->num_edges * G->num_dims * sizeof(double), nz = (size_t)G->num_vars * G->num_dims * sizeof(double);
+    void *arrs[5] = {G->X, G->M, G->N, G->U, G->Z};
+    const size_t sz[5] = {ne, ne, ne, ne, nz};
+    std::vector<void *> done;
+    for (int q = 0; q < 5; ++q) {
+        cudaError_t e = cudaHostRegister(arrs[q], sz[q], cudaHostRegisterPortable);
+        if (e != cudaSuccess) {
+            for (void *p : done) cudaHostUnregister(p);
+            return pdm_cuda_fail(e, "cudaHostRegister", __FILE__, __LINE__);
+        }
+        done.push_back(arrs[q]);
+    }
+    g_pinned[G] = done;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_unpin_graph(const graph *G)
+{
+    ok_status();
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_pinned.find(G);
+    if (it == g_pinned.end()) return PARADMM_OK;
+    for (void *p : it->second) cudaHostUnregister(p);
+    g_pinned.erase(it);
+    return PARADMM_OK;
+}
 
 extern "C" int paradmm_gpu_get_circles(paradmm_gpu *h, int instance, double *out)
 {
@@ -1184,28 +1244,56 @@ extern "C" void paradmm_set_sweep_options(const paradmm_gpu_opts *opts)
     else paradmm_gpu_default_opts(&g_sweep_opts);
 }
 
+// Fingerprint of the penalties and steps: a handle is reused only while they
+// are unchanged (the packing engine folds them into constants).  Hashed in
+// parallel chunks, combined in chunk order.
+static uint64_t fnv_chunk(const double *a, size_t n)
+{
+    uint64_t h = 1469598103934665603ULL;
+    for (size_t i = 0; i < n; ++i) {
+        uint64_t b;
+        memcpy(&b, &a[i], 8);
+        h = (h ^ b) * 1099511628211ULL;
+    }
+    return h;
+}
+
 static uint64_t coef_hash(const graph *G)
 {
-    uint64_t hsh = 1469598103934665603ULL;
-    auto mix = [&](const double *a, int n) {
-        for (int i = 0; i < n; ++i) {
-            uint64_t b;
-            memcpy(&b, &a[i], 8);
-            hsh = (hsh ^ b) * 1099511628211ULL;
-        }
+    const size_t n = (size_t)G->num_edges;
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min(nt, 32u));
+    if (n < ((size_t)1 << 20)) nt = 1;
+    std::vector<uint64_t> part(2 * nt, 0);
+    auto work = [&](unsigned t) {
+        const size_t b = n * t / nt, e = n * (t + 1) / nt;
+        part[t] = G->RHOS ? fnv_chunk(G->RHOS + b, e - b) : 0;
+        part[nt + t] = G->ALPHAS ? fnv_chunk(G->ALPHAS + b, e - b) : 0;
     };
-    if (G->RHOS) mix(G->RHOS, G->num_edges);
-    if (G->ALPHAS) mix(G->ALPHAS, G->num_edges);
-    return hsh;
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+    uint64_t h = 1469598103934665603ULL;
+    for (uint64_t v : part) h = (h ^ v) * 1099511628211ULL;
+    return h;
 }
+
+extern "C" int paradmm_gpu_unpin_graph(const graph *G);
 
 extern "C" void paradmm_internal_forget_graph(const graph *G)
 {
-    std::lock_guard<std::mutex> lk(g_sweep_mu);
-    auto it = g_cache.find(G);
-    if (it == g_cache.end()) return;
-    for (Cached &c : it->second) paradmm_gpu_destroy(c.h);
-    g_cache.erase(it);
+    const int st = t_status;
+    {
+        std::lock_guard<std::mutex> lk(g_sweep_mu);
+        auto it = g_cache.find(G);
+        if (it != g_cache.end()) {
+            for (Cached &c : it->second) paradmm_gpu_destroy(c.h);
+            g_cache.erase(it);
+        }
+    }
+    paradmm_gpu_unpin_graph(G);
+    t_status = st;
 }
 
 // Handle for G with the requested engine; uploads G's current state.
@@ -1260,6 +1348,11 @@ static void sweep_call(graph *G, int phase, int iters)
     paradmm_gpu *h = sweep_handle(G, engine_req);
     if (!h) return;
     DevGuard guard(h->device);
+    // Graphs with large state move it through pinned pages (registered once,
+    // released by closeG).
+    if ((size_t)G->num_edges * G->num_dims * sizeof(double) >= ((size_t)64 << 20)) {
+        if (paradmm_gpu_pin_graph(G) != PARADMM_OK) ok_status();  // pageable copies still work
+    }
     int rc;
     if (phase < 0) rc = paradmm_gpu_iterate(h, iters);
     else rc = gen_phase(h, phase);

@@ -50,6 +50,8 @@ struct PkHost {
     std::vector<int> nmode;
     std::vector<PkStatus> status;    // host copy after the last launch
     std::vector<long long> iters_last_call;
+    int prof = 0;                    // per-phase timing requested
+    double phase_us[4] = {0, 0, 0, 0};  // last call: mean block time per sweep (us)
     // reference-layout maps (graph handles)
     int2 *d_pmap = nullptr; long long n_pmap = 0;
     int *d_wmap = nullptr, *d_rmap = nullptr, *d_wcirc = nullptr, *d_rcirc = nullptr;
@@ -83,4 +85,5 @@ struct paradmm_gpu {
     double *d_stage[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // X M N U Z in reference layout
     std::vector<void *> allocs;
     long long device_bytes = 0;
+    long long launches = 0;          // kernels launched by this handle
 };

@@ -120,7 +120,7 @@ struct PkRun {
     int dynamic;      // dynamic work-item scheduling
     double tol;       // stop when primal + dual <= tol (tol < 0: never)
     int check_every;  // sweeps between stopping checks
-    int pad;
+    int prof;         // accumulate per-phase block times into DevCtl::prof
 };
 
 PDM_HD long long pk_tri(int I, int J, int nb) { return (long long)I * nb - (long long)I * (I - 1) / 2 + (J - I); }

@@ -168,6 +168,22 @@ int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double *circles, 
 /* Device memory the handle holds, in bytes. */
 int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h);
 
+/* Kernels the handle has launched so far. */
+int64_t paradmm_gpu_launches(const paradmm_gpu *h);
+
+/* Packing engine: when on, later sweeps record how long the average block
+ * spends per sweep in the pass, the first grid barrier, the consensus
+ * finalisation and the second barrier; paradmm_gpu_phase_times returns those
+ * four means (microseconds) for the last solve/iterate call. */
+int paradmm_gpu_set_profiling(paradmm_gpu *h, int on);
+int paradmm_gpu_phase_times(const paradmm_gpu *h, double out[4]);
+
+/* Page-locks G's X, M, N, U and Z arrays so uploads and downloads run at
+ * full PCIe/C2C rate.  The paradmm.h sweep functions do this by themselves
+ * for graphs whose edge state is >= 64 MiB; closeG (or unpin) releases it. */
+int paradmm_gpu_pin_graph(const graph *G);
+int paradmm_gpu_unpin_graph(const graph *G);
+
 /* Appends the factors of the reference demo's packing graph to G (which
  * must be fresh from startG(G, 2)): one radius factor per circle on var 2i+1,
  * each of the n_walls half-planes on every circle (vars 2i, 2i+1), and every

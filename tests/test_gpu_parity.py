@@ -131,16 +131,38 @@ def test_packing_teacher_forced_one_sweep(bw):
     print(f"teacher-forced worst max|diff| = {worst:.3e}")
 
 
-def test_packing_free_running_20():
+def test_packing_free_running_from_init():
+    """Free-running from the random init.  The early phase is chaotic: an
+    FP32 re-evaluation of the same formulas on the CPU leaves 1e-4 of the
+    FP64 reference at iterate 9 for this instance, so the horizon is 8."""
     N = 120
     pg, orc, _ = problem(N, 4)
     with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
-        for k in range(20):
+        for k in range(8):
             h.iterate(1)
             h.download(pg.G)
             orc.sweep()
             d = maxdiff(pg.G.state(), orc.state())
             assert d <= TOL_F32, f"iterate {k + 1}: max diff {d}"
+
+
+def test_packing_free_running_near_fixed_point():
+    """50 free-running FP32 sweeps from the reference's iterate 1500."""
+    N = 80
+    pg, orc, _ = problem(N, 6)
+    orc.run(1500, trace=False)
+    for k, v in orc.state().items():
+        pg.G.arr(k)[:] = v
+    worst = 0.0
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
+        for k in range(50):
+            h.iterate(1)
+            h.download(pg.G)
+            orc.sweep()
+            d = maxdiff(pg.G.state(), orc.state())
+            worst = max(worst, d)
+            assert d <= TOL_F32, f"iterate {1500 + k + 1}: max diff {d}"
+    print(f"near-fixed-point free-running worst max|diff| = {worst:.3e}")
 
 
 def test_dropin_updateG_runs_packing_engine():
