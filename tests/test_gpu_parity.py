@@ -166,6 +166,10 @@ def test_packing_free_running_near_fixed_point():
 
 
 def test_dropin_updateG_runs_packing_engine():
+    """updateG / updateGOpenMP (default engine: packing FP32) against the
+    reference: 5 single sweeps from the init, then 30 sweeps in one call
+    from a near-fixed-point state (the early phase is too chaotic for 35
+    free-running FP32 sweeps, see test_packing_free_running_from_init)."""
     pg, orc, _ = problem(40, 2)
     lib = eb.load()
     lib.paradmm_set_sweep_options(None)
@@ -174,9 +178,13 @@ def test_dropin_updateG_runs_packing_engine():
         assert eb.last_status() == eb.OK, eb.last_error()
         orc.sweep()
     assert maxdiff(pg.G.state(), orc.state()) <= TOL_F32
+    orc.run(1500, trace=False)
+    for k, v in orc.state().items():
+        pg.G.arr(k)[:] = v
     lib.updateGOpenMP(C.byref(pg.G), 30, 8)
+    assert eb.last_status() == eb.OK, eb.last_error()
     orc.run(30, trace=False)
-    assert maxdiff(pg.G.state(), orc.state()) <= 1e-3  # 35 free-running FP32 sweeps
+    assert maxdiff(pg.G.state(), orc.state()) <= TOL_F32
     lib.closeG(C.byref(pg.G))
 
 
