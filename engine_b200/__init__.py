@@ -143,6 +143,9 @@ _SIGS = {
     "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "paradmm_gpu_pin_graph": (C.c_int, [C.POINTER(Graph)]),
     "paradmm_gpu_unpin_graph": (C.c_int, [C.POINTER(Graph)]),
+    "paradmm_noalloc_state_bytes": (C.c_int64, [C.c_int, C.c_int]),
+    "paradmm_gpu_packing_iterate_noalloc": (C.c_int, [C.POINTER(PackingDesc), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                      C.c_double, C.POINTER(Stats), C.c_int, C.c_void_p]),
     "paradmm_last_status": (C.c_int, []),
     "paradmm_last_error_string": (C.c_char_p, []),
     "paradmm_set_sweep_options": (None, [C.POINTER(Opts)]),

@@ -30,6 +30,7 @@ CU_SOURCES = {
     "engine.cu": [],
     "packing_kernels.cu": [],
     "generic_kernels.cu": ["-fmad=false"],
+    "noalloc.cu": [],
 }
 C_SOURCES = {"graph.c": ["-O2", "-std=gnu11", "-fPIC", "-ffp-contract=off"]}
 

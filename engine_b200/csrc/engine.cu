@@ -51,6 +51,7 @@ extern "C" int paradmm_last_status(void) { return t_status; }
 extern "C" const char *paradmm_last_error_string(void) { return t_msg; }
 
 static inline void ok_status() { t_status = PARADMM_OK; }
+void pdm_clear_status() { t_status = PARADMM_OK; }
 
 struct DevGuard {
     int prev = -1;

@@ -12,6 +12,7 @@
 #include "packing.cuh"
 
 int pdm_set_error(int status, const char *fmt, ...);
+void pdm_clear_status();  // marks the calling thread's last call as successful
 
 // Result of classifying a host graph.
 struct GraphInfo {

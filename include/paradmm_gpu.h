@@ -195,6 +195,47 @@ int paradmm_gpu_unpin_graph(const graph *G);
  * (packing/host.c:299-335). */
 int paradmm_add_packing_factors(graph *G, int n_circles, int n_walls, double *walls, double *exponent, int order);
 
+/* ---- allocation-free packing sweeps ----
+ *
+ * Some callers cannot allocate device memory while they run: services that
+ * reserve their whole device-memory budget up front and forbid any later
+ * cudaMalloc, and latency-critical loops (a planner re-solving a packing
+ * every control tick, for instance), where cudaMalloc/cudaFree can
+ * synchronise the device and stall every other stream.  This entry point
+ * serves them: it allocates nothing.  (It has no counterpart in the
+ * reference, which allocates per factor.)
+ *
+ * It runs `sweeps` fused sweeps (stopping early once primal + dual <= tol,
+ * tol < 0: never) of ONE packing instance described by `desc` (desc->init
+ * is ignored).  The caller passes, in device memory it owns:
+ *   d_circles  n_circles x [cx, cy, r] doubles: the consensus, read at the
+ *              start and written back at the end;
+ *   d_state    paradmm_noalloc_state_bytes(n_circles, n_walls) bytes: the
+ *              FP32 edge state in the engine's layout (opaque to the
+ *              caller).  With init_state = 1 it is first set to the plain
+ *              start X_e = Z_v(e), U = 0; with init_state = 0 it must hold
+ *              the state a previous call left, so consecutive calls continue
+ *              one solve.
+ * All scratch (tables, consensus partial sums, residual slots, barrier
+ * control) lives in one fixed array of PARADMM_NOALLOC_SCRATCH_BYTES inside
+ * this library, present on every GPU that loads it until the process exits.
+ * Limits: n_circles <= PARADMM_NOALLOC_MAX_CIRCLES, n_walls <=
+ * PARADMM_NOALLOC_MAX_WALLS; larger problems are rejected with PARADMM_EINVAL.
+ * The first call on a device looks up that array's device address (a
+ * one-time set-up); make that first call before any stream capture.  Every
+ * call reuses the same array and overwrites what the previous call left, so
+ * calls whose work overlaps on the GPU (other threads or streams) race: run
+ * them one after another.  `stream` is a cudaStream_t (NULL: the default
+ * stream); the call returns after the work on it has finished.  stats may be
+ * NULL; its device_ms is host-measured. */
+#define PARADMM_NOALLOC_MAX_CIRCLES 512
+#define PARADMM_NOALLOC_MAX_WALLS 8
+#define PARADMM_NOALLOC_SCRATCH_BYTES (512 * 1024)
+int64_t paradmm_noalloc_state_bytes(int n_circles, int n_walls);
+int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *desc, double *d_circles, void *d_state,
+                                        int init_state, int sweeps, double tol, paradmm_stats *stats,
+                                        int device, void *stream);
+
 /* ---- errors ---- */
 int paradmm_last_status(void);
 const char *paradmm_last_error_string(void);
