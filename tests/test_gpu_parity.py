@@ -268,3 +268,33 @@ def test_nonfinite_is_reported():
         s = h.solve(50, -1.0)
         assert s["status"] == eb.ENONFINITE
         assert eb.last_status() == eb.ENONFINITE
+
+
+# ------------------------------------------------------ golden fixtures (GPU)
+import glob as _glob  # noqa: E402
+import os as _os  # noqa: E402
+
+_GOLDEN = sorted(_glob.glob(_os.path.join(_os.path.dirname(__file__), "golden", "*.npz")))
+
+
+@pytest.mark.parametrize("path", _GOLDEN, ids=[_os.path.basename(p) for p in _GOLDEN])
+def test_generic_f64_reproduces_golden(path):
+    """The exact engine reproduces the reference's own outputs bit for bit."""
+    g = np.load(path)
+    N = int(g["N"])
+    pg = eb.PackingGraph(N, g["walls"], 2.0, order=int(g["order"]))
+    lib = eb.load()
+    lib.initialize_X_N_Z_M_U_zeros(C.byref(pg.G))
+    lib.initialize_RHOS_APHAS(C.byref(pg.G), float(g["rho"]), float(g["alpha"]))
+    pg.G.arr("RHOS")[:] = g["RHOS"]
+    for k in ("X", "M", "N", "U", "Z"):
+        pg.G.arr(k)[:] = g[f"init_{k}"]
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_GENERIC_F64) as h:
+        done = 0
+        for s in g["snaps"]:
+            h.iterate(int(s) - done)
+            done = int(s)
+            h.download(pg.G)
+            st = pg.G.state()
+            for k in ("X", "M", "N", "U", "Z"):
+                assert np.array_equal(st[k], g[f"it{s}_{k}"]), f"{k} at sweep {s}"
