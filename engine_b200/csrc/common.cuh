@@ -20,14 +20,16 @@ enum : int {
 // Control block of one persistent launch: grid barrier, error flag, work
 // counters.  Lives in device memory owned by the handle; zeroed before each
 // launch.
+#define PDM_BAR_GROUPS 16
 struct DevCtl {
-    unsigned int bar_count;   // arrivals at the current barrier
+    unsigned int bar_count;   // arrivals of group leaders at the current barrier
     unsigned int bar_gen;     // barrier generation (bumped by the last arrival)
     int err;                  // DEV_* error, first writer wins
     int n_active;             // instances still iterating
     unsigned int item_ctr[2]; // dynamic work counters, one per iteration parity
     unsigned int pad[2];      // pad[0]: sweeps completed by the launch
     unsigned long long prof[4];  // optional: summed block time in pass, barrier 1, finalise, barrier 2 (ns)
+    unsigned int grp_count[PDM_BAR_GROUPS][32];  // per-group arrivals, one 128-B line each
 };
 
 // Barrier waits give up after this long; the kernel then records
@@ -65,9 +67,12 @@ PDM_D unsigned atom_add_acq_rel_u32(unsigned *p, unsigned v)
 
 PDM_D int ld_volatile_i32(const int *p) { return *(const volatile int *)p; }
 
-// Grid-wide barrier for a cooperative (co-resident) launch.  Every wait is
-// bounded by PDM_BARRIER_TIMEOUT_NS and PDM_BARRIER_MAX_POLLS; on timeout, or
-// when another block has already recorded an error, it returns false and the
+// Grid-wide barrier for a cooperative (co-resident) launch.  Blocks arrive
+// on one of PDM_BAR_GROUPS group counters (separate cache lines); the last
+// block of each group arrives on the root counter, and the last root arrival
+// releases everyone by bumping the generation.  Every wait is bounded by
+// PDM_BARRIER_TIMEOUT_NS and PDM_BARRIER_MAX_POLLS; on timeout, or when
+// another block has already recorded an error, it returns false and the
 // caller leaves its loop.  All threads of the block get the same answer.
 PDM_D bool grid_barrier(DevCtl *ctl)
 {
@@ -75,14 +80,25 @@ PDM_D bool grid_barrier(DevCtl *ctl)
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        const unsigned ngroups = nblocks < PDM_BAR_GROUPS ? nblocks : PDM_BAR_GROUPS;
+        const unsigned grp = bid % ngroups;
+        const unsigned in_grp = (nblocks - grp + ngroups - 1) / ngroups;  // blocks of this group
         const unsigned gen = ld_acquire_u32(&ctl->bar_gen);
         __threadfence();
-        const unsigned arrived = atom_add_acq_rel_u32(&ctl->bar_count, 1u);
         int ok = 1;
-        if (arrived == nblocks - 1) {
-            *(volatile unsigned *)&ctl->bar_count = 0u;
-            st_release_u32(&ctl->bar_gen, gen + 1u);
-        } else {
+        bool releaser = false;
+        const unsigned a = atom_add_acq_rel_u32(&ctl->grp_count[grp][0], 1u);
+        if (a == in_grp - 1) {
+            *(volatile unsigned *)&ctl->grp_count[grp][0] = 0u;
+            const unsigned r = atom_add_acq_rel_u32(&ctl->bar_count, 1u);
+            if (r == ngroups - 1) {
+                *(volatile unsigned *)&ctl->bar_count = 0u;
+                st_release_u32(&ctl->bar_gen, gen + 1u);
+                releaser = true;
+            }
+        }
+        if (!releaser) {
             const uint64_t t0 = globaltimer_ns();
             uint64_t polls = 0;
             while (ld_acquire_u32(&ctl->bar_gen) == gen) {
@@ -92,7 +108,7 @@ PDM_D bool grid_barrier(DevCtl *ctl)
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
         if (ld_volatile_i32(&ctl->err) != DEV_OK) ok = 0;

@@ -339,12 +339,12 @@ static int add_items(PkHost &P, int inst_id, int N, int nb)
     return n;
 }
 
+// Tile side: 64 circles (two columns per lane) or 128 (four).
 static int pick_V(const paradmm_gpu_opts &o, int maxN)
 {
-    if (o.block_width == 32) return 1;
-    if (o.block_width == 64) return 2;
     if (o.block_width == 128) return 4;
-    if (maxN <= 160) return 1;
+    if (o.block_width == 32 || o.block_width == 64) return 2;
+    (void)maxN;
     return 2;
 }
 
@@ -381,10 +381,18 @@ static int pk_finalize_build(paradmm_gpu *h)
         std::stable_sort(claim.begin(), claim.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     }
 
+    // consensus items: one per circle block of every instance
+    std::vector<int2> fin;
+    for (int i = 0; i < P.n_inst; ++i) {
+        P.inst[i].fin_base = (int)fin.size();
+        for (int b = 0; b < P.inst[i].nb; ++b) fin.push_back(make_int2(i, b));
+    }
+
     PkDev &D = P.D;
     D.n_inst = P.n_inst;
     D.n_items = P.n_items;
     D.n_circ = P.n_circ;
+    D.n_fin = (int)fin.size();
     int rc;
     if ((rc = dput(h, (PkInst **)&D.inst, P.inst))) return rc;
     if ((rc = dput(h, (int4 **)&D.items, P.items))) return rc;
@@ -400,10 +408,13 @@ static int pk_finalize_build(paradmm_gpu *h)
         if ((rc = dput(h, &D.Z, z))) return rc;
     }
     if ((rc = dalloc(h, (void **)&D.local_part, sizeof(double4) * (size_t)P.n_circ))) return rc;
-    if ((rc = dalloc(h, (void **)&D.circ_dual, sizeof(double) * 2 * (size_t)P.n_circ))) return rc;
+    if ((rc = dput(h, (int2 **)&D.fin_items, fin))) return rc;
     if ((rc = dalloc(h, (void **)&D.item_primal, sizeof(double) * 2 * (size_t)P.n_items))) return rc;
-    PDM_CUDA(cudaMemset(D.circ_dual, 0, sizeof(double) * 2 * (size_t)P.n_circ));
+    if ((rc = dalloc(h, (void **)&D.blk_primal, sizeof(double) * 4 * (size_t)D.n_fin))) return rc;
+    if ((rc = dalloc(h, (void **)&D.blk_dual, sizeof(double) * 4 * (size_t)D.n_fin))) return rc;
     PDM_CUDA(cudaMemset(D.item_primal, 0, sizeof(double) * 2 * (size_t)P.n_items));
+    PDM_CUDA(cudaMemset(D.blk_primal, 0, sizeof(double) * 4 * (size_t)D.n_fin));
+    PDM_CUDA(cudaMemset(D.blk_dual, 0, sizeof(double) * 4 * (size_t)D.n_fin));
     if ((rc = dalloc(h, (void **)&D.status, sizeof(PkStatus) * (size_t)P.n_inst))) return rc;
     if ((rc = dput(h, (float4 **)&D.wall_vp, P.wall_vp))) return rc;
     if ((rc = dput(h, (float4 **)&D.wall_coef, P.wall_coef))) return rc;
@@ -423,6 +434,14 @@ static int pk_finalize_build(paradmm_gpu *h)
         return pdm_set_error(PARADMM_ECUDA, "packing kernel cannot be resident on this device");
     if (h->opts.ctas_per_sm > 0) bps = std::min(bps, h->opts.ctas_per_sm);
     P.grid = h->num_sms * bps;
+    // Small problems: fewer CTAs (barrier cost grows with the CTA count and
+    // there is no work for the rest).
+    {
+        int fin_n = D.n_fin;
+        const int want = std::max(std::max(P.n_items, fin_n), P.n_inst);
+        if (want < P.grid) P.grid = std::max(std::min(P.grid, h->num_sms), ((want + 31) / 32) * 32);
+        if (P.grid > h->num_sms * bps) P.grid = h->num_sms * bps;
+    }
     P.upload_iter.assign(P.n_inst, 0);
     P.nmode.assign(P.n_inst, 0);
     P.status.assign(P.n_inst, PkStatus{});
@@ -709,7 +728,7 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
             PkStatus &s = st[i];
             s = P.status[i];
             s.last_iter = done[i] ? it0 - 1 : LLONG_MAX;
-            s.check_from = it0 + 1;
+            s.check_from = it0 + 2;
             s.converged = 0;
             s.nonfinite = 0;
             s.nmode = P.nmode[i];

@@ -42,9 +42,11 @@ struct NaLayout {
     static constexpr size_t col_part = row_part + na_al(sizeof(double4) * NA_TILES * NA_BW);
     static constexpr size_t Z = col_part + na_al(sizeof(double4) * NA_TILES * NA_BW);
     static constexpr size_t local_part = Z + na_al(sizeof(double4) * NA_MAX_CIRCLES);
-    static constexpr size_t circ_dual = local_part + na_al(sizeof(double4) * NA_MAX_CIRCLES);
-    static constexpr size_t item_primal = circ_dual + na_al(sizeof(double) * 2 * NA_MAX_CIRCLES);
-    static constexpr size_t status = item_primal + na_al(sizeof(double) * 2 * NA_ITEMS);
+    static constexpr size_t fin_items = local_part + na_al(sizeof(double4) * NA_MAX_CIRCLES);
+    static constexpr size_t item_primal = fin_items + na_al(sizeof(int2) * NA_NB);
+    static constexpr size_t blk_primal = item_primal + na_al(sizeof(double) * 2 * NA_ITEMS);
+    static constexpr size_t blk_dual = blk_primal + na_al(sizeof(double) * 4 * NA_NB);
+    static constexpr size_t status = blk_dual + na_al(sizeof(double) * 4 * NA_NB);
     static constexpr size_t wall_vp = status + na_al(sizeof(PkStatus));
     static constexpr size_t wall_coef = wall_vp + na_al(sizeof(float4) * NA_WALLS);
     static constexpr size_t wall_rho = wall_coef + na_al(sizeof(float4) * NA_WALLS);
@@ -70,6 +72,7 @@ static int g_na_grid[NA_MAX_DEVICES];
 static PkInst s_inst;
 static int4 s_items[NA_ITEMS];
 static int s_claim[NA_ITEMS];
+static int2 s_fin[NA_NB];
 static PkCircle s_circ[NA_MAX_CIRCLES];
 static float4 s_wall_vp[NA_WALLS], s_wall_coef[NA_WALLS];
 static double2 s_wall_rho[NA_WALLS];
@@ -159,6 +162,8 @@ static void na_tables(const paradmm_packing_desc &d, int *n_items_out)
     for (int c0 = 0; c0 < N; c0 += PK_THREADS) s_items[n++] = make_int4(0, 1, c0, std::min(PK_THREADS, N - c0));
     I.item_base = 0;
     I.n_items = n;
+    I.fin_base = 0;
+    for (int b = 0; b < I.nb; ++b) s_fin[b] = make_int2(0, b);
     for (int q = 0; q < n; ++q) s_claim[q] = q;  // tiles come first: largest first already
     *n_items_out = n;
 }
@@ -207,8 +212,11 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     D.col_part = (double4 *)(base + NaLayout::col_part);
     D.Z = (double4 *)(base + NaLayout::Z);
     D.local_part = (double4 *)(base + NaLayout::local_part);
-    D.circ_dual = (double *)(base + NaLayout::circ_dual);
+    D.fin_items = (const int2 *)(base + NaLayout::fin_items);
+    D.n_fin = s_inst.nb;
     D.item_primal = (double *)(base + NaLayout::item_primal);
+    D.blk_primal = (double *)(base + NaLayout::blk_primal);
+    D.blk_dual = (double *)(base + NaLayout::blk_dual);
     D.status = (PkStatus *)(base + NaLayout::status);
     D.wall_vp = (const float4 *)(base + NaLayout::wall_vp);
     D.wall_coef = (const float4 *)(base + NaLayout::wall_coef);
@@ -237,8 +245,10 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     }
     PDM_CUDA(cudaMemcpyAsync((void *)D.rad_coef, s_rad_coef, sizeof(float4) * N, cudaMemcpyHostToDevice, s));
     PDM_CUDA(cudaMemcpyAsync((void *)D.rad_rho, s_rad_rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    PDM_CUDA(cudaMemsetAsync(D.circ_dual, 0, sizeof(double) * 2 * N, s));
+    PDM_CUDA(cudaMemcpyAsync((void *)D.fin_items, s_fin, sizeof(int2) * s_inst.nb, cudaMemcpyHostToDevice, s));
     PDM_CUDA(cudaMemsetAsync(D.item_primal, 0, sizeof(double) * 2 * n_items, s));
+    PDM_CUDA(cudaMemsetAsync(D.blk_primal, 0, sizeof(double) * 4 * s_inst.nb, s));
+    PDM_CUDA(cudaMemsetAsync(D.blk_dual, 0, sizeof(double) * 4 * s_inst.nb, s));
     // consensus: caller's [cx, cy, r] rows -> the kernel's (cx, cy, r, -) rows
     PDM_CUDA(cudaMemcpy2DAsync(D.Z, sizeof(double4), d_circles, 3 * sizeof(double), 3 * sizeof(double), N,
                                cudaMemcpyDeviceToDevice, s));
@@ -256,7 +266,7 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         const int chunk = (int)std::min<long long>(left, 8192);
         memset(&s_status, 0, sizeof s_status);
         s_status.last_iter = LLONG_MAX;
-        s_status.check_from = it0 + 1;
+        s_status.check_from = it0 + 2;
         s_status.resid_iter = -1;
         s_status.primal = s_status.dual = NAN;
         memset(&s_ctl, 0, sizeof s_ctl);

@@ -48,7 +48,7 @@ struct PkInst {
     int circle_base;        // global index of the instance's circle 0
     int item_base;          // first work item
     int n_items;            // work items (pair tiles + circle blocks)
-    int pad0;
+    int fin_base;           // first consensus item (one per circle block)
     long long tile_base;    // global index of tile (0, 0)
     float alpha[4];         // pair edge steps by position (c_i, r_i, c_j, r_j)
     float A1, A2, B2m1, C1; // pair prox coefficients (see pair_prox)
@@ -70,9 +70,9 @@ struct PkCircle {
     int pad[3];
 };
 
-// Work item: x = instance, y = kind (0 pair tile, 1 circle block),
-// kind 0: z = I, w = J (block indices); kind 1: z = first circle, w = count.
-// (int4)
+// Work item of the pass: x = instance, y = kind (0 pair tile, 1 circle
+// block), kind 0: z = I, w = J (block indices); kind 1: z = first circle,
+// w = count (int4).  Consensus item: x = instance, y = circle block (int2).
 
 // Per-instance run status, written by the kernel.
 struct PkStatus {
@@ -98,8 +98,11 @@ struct PkDev {
     double4 *col_part;       // [tile][BW] same for the column circle
     double4 *Z;              // [circle] consensus (cx, cy, r, -)
     double4 *local_part;     // [circle] rho-weighted wall + radius contributions
-    double *circ_dual;       // [2][n_circ] dual-residual partials by parity
-    double *item_primal;     // [2][n_items] primal-residual partials by parity
+    const int2 *fin_items;   // [n_fin] consensus items (instance, circle block)
+    int n_fin, pad2;
+    double *item_primal;     // [2][n_items] primal-residual partials by sweep parity
+    double *blk_primal;      // [4][n_fin] per consensus item, by sweep index mod 4
+    double *blk_dual;        // [4][n_fin]
     PkStatus *status;        // [n_inst]
     // walls (sorted by circle)
     const float4 *wall_vp;   // v_x, v_y, p_x, p_y

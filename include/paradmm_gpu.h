@@ -105,9 +105,12 @@ int paradmm_gpu_upload(paradmm_gpu *h, const graph *G);
 /* Runs n full sweeps (updateG semantics). */
 int paradmm_gpu_iterate(paradmm_gpu *h, int n);
 
-/* Runs up to maxiter sweeps, stopping once primal + dual <= tol (tol <= 0:
- * never).  The check lags one sweep: the state returned is one sweep past the
- * first iterate whose residuals met the tolerance.  stats may be NULL. */
+/* Runs up to maxiter sweeps, stopping once primal + dual <= tol (tol < 0:
+ * never).  Packing engine: the residuals of iterate k are reduced on the
+ * device while sweeps k+1 and k+2 run, so the state returned is two sweeps
+ * past the first iterate whose residuals met the tolerance (the stats give
+ * that iterate's residuals); the generic engine stops at that iterate.
+ * stats may be NULL. */
 int paradmm_gpu_solve(paradmm_gpu *h, int maxiter, double tol, paradmm_stats *stats);
 
 /* Writes X, M, N, U and Z of the current iterate into G (reference layout,
