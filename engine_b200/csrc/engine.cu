@@ -442,6 +442,24 @@ static int pk_finalize_build(paradmm_gpu *h)
         if (want < P.grid) P.grid = std::max(std::min(P.grid, h->num_sms), ((want + 31) / 32) * 32);
         if (P.grid > h->num_sms * bps) P.grid = h->num_sms * bps;
     }
+    // Schedule: batches of small instances run one CTA per instance (no grid
+    // barrier); a few or large instances share the grid-wide persistent loop.
+    {
+        int maxN = 0;
+        for (const PkInst &I : P.inst) maxN = std::max(maxN, I.N);
+        const int req = h->opts.schedule;
+        const bool small = maxN <= 1024;
+        if (req == PARADMM_SCHEDULE_INSTANCE && small) P.schedule = PARADMM_SCHEDULE_INSTANCE;
+        else if (req == PARADMM_SCHEDULE_GRID || !small) P.schedule = PARADMM_SCHEDULE_GRID;
+        else P.schedule = P.n_inst >= 8 ? PARADMM_SCHEDULE_INSTANCE : PARADMM_SCHEDULE_GRID;
+        std::vector<int> order(P.n_inst);
+        for (int i = 0; i < P.n_inst; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return P.inst[a].N > P.inst[b].N; });
+        if ((rc = dput(h, &P.d_order, order))) return rc;
+        int ib = 0;
+        if (pk_instances_blocks_per_sm(P.V, P.stream_hint, &ib) != cudaSuccess || ib < 1) ib = 1;
+        P.inst_grid = h->num_sms * ib;
+    }
     P.upload_iter.assign(P.n_inst, 0);
     P.nmode.assign(P.n_inst, 0);
     P.status.assign(P.n_inst, PkStatus{});
@@ -711,10 +729,56 @@ static int pk_download_graph(paradmm_gpu *h, graph *G)
 // PK_SWEEPS_PER_LAUNCH sweeps).  Per-instance iteration counts land in
 // P.iters_last_call, statuses in P.status.
 #define PK_SWEEPS_PER_LAUNCH 8192
+static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_every, double *ms)
+{
+    PkHost &P = *h->pk;
+    const long long it0 = P.it_next;
+    std::vector<PkStatus> st(P.n_inst);
+    for (int i = 0; i < P.n_inst; ++i) {
+        PkStatus &s = st[i];
+        s = P.status[i];
+        s.last_iter = LLONG_MAX;
+        s.check_from = it0 + 1;
+        s.converged = 0;
+        s.nonfinite = 0;
+        s.nmode = P.nmode[i];
+    }
+    PDM_CUDA(cudaMemcpyAsync(P.D.status, st.data(), sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
+    DevCtl c{};
+    PDM_CUDA(cudaMemcpyAsync(h->ctl, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
+    PkRun R{};
+    R.it0 = it0;
+    R.n_iter = (int)std::min<long long>(n, INT_MAX);
+    R.dynamic = 0;
+    R.tol = tol;
+    R.check_every = check_every < 1 ? 1 : check_every;
+    PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
+    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, &h->ctl->item_ctr[0], P.inst_grid, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "per-instance packing launch", __FILE__, __LINE__);
+    ++h->launches;
+    PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(st.data(), P.D.status, sizeof(PkStatus) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    float t = 0;
+    cudaEventElapsedTime(&t, h->ev0, h->ev1);
+    if (ms) *ms = t;
+    int rc = PARADMM_OK;
+    for (int i = 0; i < P.n_inst; ++i) {
+        const long long ran = st[i].last_iter - it0 + 1;
+        P.iters_last_call[i] = ran > 0 ? ran : 0;
+        if (ran > 0) P.nmode[i] = 0;
+        P.status[i] = st[i];
+        if (st[i].nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
+    }
+    P.it_next = it0 + n;
+    return rc;
+}
+
 static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, double *ms)
 {
     PkHost &P = *h->pk;
     std::fill(P.iters_last_call.begin(), P.iters_last_call.end(), 0LL);
+    if (P.schedule == PARADMM_SCHEDULE_INSTANCE) return pk_run_instances(h, n, tol, check_every, ms);
     std::vector<char> done(P.n_inst, 0);
     double total_ms = 0;
     long long left = n;
@@ -1246,7 +1310,7 @@ extern "C" void paradmm_gpu_destroy(paradmm_gpu *h)
 // paradmm.h sweep functions (GPU-backed drop-ins)
 // ===========================================================================
 static std::mutex g_sweep_mu;
-static paradmm_gpu_opts g_sweep_opts = {0, PARADMM_ENGINE_AUTO, 0, 0, 1, {0}};
+static paradmm_gpu_opts g_sweep_opts = {0, PARADMM_ENGINE_AUTO, 0, 0, 1, PARADMM_SCHEDULE_AUTO, {0}};
 
 struct Cached {
     paradmm_gpu *h = nullptr;

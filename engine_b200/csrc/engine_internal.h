@@ -51,6 +51,9 @@ struct PkHost {
     std::vector<int> nmode;
     std::vector<PkStatus> status;    // host copy after the last launch
     std::vector<long long> iters_last_call;
+    int schedule = PARADMM_SCHEDULE_GRID;  // resolved schedule
+    int inst_grid = 0;               // CTAs of the per-instance schedule
+    int *d_order = nullptr;          // instances, largest first (per-instance schedule)
     int prof = 0;                    // per-phase timing requested
     double phase_us[4] = {0, 0, 0, 0};  // last call: mean block time per sweep (us)
     // reference-layout maps (graph handles)

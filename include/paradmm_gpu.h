@@ -72,8 +72,16 @@ typedef struct paradmm_gpu_opts {
     int block_width;  /* packing engine: circles per tile side (32, 64, 128); 0 = tuned */
     int ctas_per_sm;  /* packing engine: resident CTAs per SM; 0 = tuned       */
     int check_every;  /* sweeps between residual-based stopping checks; 0 = 1  */
-    int reserved[8];
+    int schedule;     /* packing engine: PARADMM_SCHEDULE_*                      */
+    int reserved[7];
 } paradmm_gpu_opts;
+
+/* How the packing engine spreads a handle's instances over the GPU. */
+enum {
+    PARADMM_SCHEDULE_AUTO = 0,     /* per-instance CTAs for batches of small instances, else grid-wide */
+    PARADMM_SCHEDULE_GRID = 1,     /* every CTA works on every instance; grid barrier per sweep        */
+    PARADMM_SCHEDULE_INSTANCE = 2  /* one CTA per instance at a time, no grid barrier (N <= 1024)      */
+};
 
 typedef struct paradmm_stats {
     int64_t iterations;   /* sweeps performed by the call                       */

@@ -300,10 +300,12 @@ def test_generic_f64_reproduces_golden(path):
                 assert np.array_equal(st[k], g[f"it{s}_{k}"]), f"{k} at sweep {s}"
 
 
-def test_batched_solve_with_retiring_instances_equals_single():
+@pytest.mark.parametrize("schedule", [eb.SCHEDULE_GRID, eb.SCHEDULE_INSTANCE])
+def test_batched_solve_with_retiring_instances_equals_single(schedule):
     """Instances of a batch stop on their own residual; the ones still
     iterating must evolve exactly as if solved alone (same sweeps, same
-    residuals), however many of their neighbours have retired."""
+    circles), however many of their neighbours have retired -- on both
+    schedules (grid-wide persistent loop, one CTA per instance)."""
     rng = np.random.default_rng(11)
     descs = []
     for i in range(96):
@@ -311,14 +313,14 @@ def test_batched_solve_with_retiring_instances_equals_single():
         asp = float(rng.uniform(1, 2))
         descs.append(dict(n_circles=N, walls=eb.box_walls(asp, 1.0), exponent=EXP, rho=RHO, rho_radius=RHO_R,
                           alpha=ALPHA, init=eb.seeded_circles(N, asp, 1.0, 0.05, 500 + i)))
-    with eb.Handle.packing(descs) as hb:
+    with eb.Handle.packing(descs, schedule=schedule) as hb:
         hb.solve(8000, 1e-5)
         batched = hb.instance_stats()
         circ = [hb.circles(i, d["n_circles"]) for i, d in enumerate(descs)]
     n_conv = sum(s["converged"] for s in batched)
     assert n_conv >= len(descs) // 2  # many retire early: that is the case under test
     for i in range(0, len(descs), 5):
-        with eb.Handle.packing([descs[i]]) as h1:
+        with eb.Handle.packing([descs[i]], schedule=schedule) as h1:
             h1.solve(8000, 1e-5)
             single = h1.instance_stats()[0]
             c1 = h1.circles(0, descs[i]["n_circles"])
