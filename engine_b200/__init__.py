@@ -69,7 +69,7 @@ class Graph(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("engine", C.c_int), ("block_width", C.c_int), ("ctas_per_sm", C.c_int),
-                ("check_every", C.c_int), ("schedule", C.c_int), ("reserved", C.c_int * 7)]
+                ("check_every", C.c_int), ("schedule", C.c_int), ("cluster_size", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class Stats(C.Structure):
@@ -140,6 +140,7 @@ _SIGS = {
     "paradmm_gpu_warm_start": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     "paradmm_gpu_device_bytes": (C.c_int64, [C.c_void_p]),
     "paradmm_gpu_launches": (C.c_int64, [C.c_void_p]),
+    "paradmm_gpu_instance_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "paradmm_gpu_pin_graph": (C.c_int, [C.POINTER(Graph)]),
@@ -401,6 +402,15 @@ class Handle:
 
     def device_bytes(self) -> int:
         return self.lib.paradmm_gpu_device_bytes(self.ptr)
+
+    def instance_times(self) -> tuple[np.ndarray, np.ndarray]:
+        """Per-instance schedule: (start_ms, stop_ms) of every instance in the last call."""
+        n = self.instances()
+        b = np.zeros(n)
+        e = np.zeros(n)
+        check(self.lib.paradmm_gpu_instance_times(self.ptr, b.ctypes.data_as(C.POINTER(C.c_double)),
+                                                  e.ctypes.data_as(C.POINTER(C.c_double))))
+        return b, e
 
     def launches(self) -> int:
         return self.lib.paradmm_gpu_launches(self.ptr)

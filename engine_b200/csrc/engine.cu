@@ -456,9 +456,23 @@ static int pk_finalize_build(paradmm_gpu *h)
         for (int i = 0; i < P.n_inst; ++i) order[i] = i;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return P.inst[a].N > P.inst[b].N; });
         if ((rc = dput(h, &P.d_order, order))) return rc;
+        // Large instances are the critical path of a batch: they get a whole
+        // cluster each; the rest run one per CTA.
+        int cl = h->opts.cluster_size;
+        if (cl != 1 && cl != 2 && cl != 4 && cl != 8) cl = 4;
+        int nclu = 0;
+        while (cl > 1 && (pk_instances_max_clusters(P.V, P.stream_hint, cl, &nclu) != cudaSuccess || nclu < 1)) {
+            cudaGetLastError();
+            cl /= 2;
+        }
+        P.cluster = cl;
         int ib = 0;
         if (pk_instances_blocks_per_sm(P.V, P.stream_hint, &ib) != cudaSuccess || ib < 1) ib = 1;
-        P.inst_grid = h->num_sms * ib;
+        P.inst_grid = cl > 1 ? nclu * cl : h->num_sms * ib;
+        P.coop_min_n = h->opts.reserved[0] > 0 ? h->opts.reserved[0] : 200;
+        P.n_coop = 0;
+        if (cl > 1)
+            for (int q = 0; q < P.n_inst && P.inst[order[q]].N >= P.coop_min_n; ++q) P.n_coop = q + 1;
     }
     P.upload_iter.assign(P.n_inst, 0);
     P.nmode.assign(P.n_inst, 0);
@@ -742,6 +756,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
         s.converged = 0;
         s.nonfinite = 0;
         s.nmode = P.nmode[i];
+        s.t_begin_ns = s.t_end_ns = 0;
     }
     PDM_CUDA(cudaMemcpyAsync(P.D.status, st.data(), sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
     DevCtl c{};
@@ -753,7 +768,8 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     R.tol = tol;
     R.check_every = check_every < 1 ? 1 : check_every;
     PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
-    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, &h->ctl->item_ctr[0], P.inst_grid, h->stream);
+    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, &h->ctl->item_ctr[0],
+                                        P.inst_grid, P.cluster, h->stream);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "per-instance packing launch", __FILE__, __LINE__);
     ++h->launches;
     PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
@@ -1201,6 +1217,21 @@ extern "C" int paradmm_gpu_instances(const paradmm_gpu *h) { return !h ? 0 : (h-
 extern "C" int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h) { return h ? h->device_bytes : 0; }
 extern "C" int64_t paradmm_gpu_launches(const paradmm_gpu *h) { return h ? h->launches : 0; }
 
+extern "C" int paradmm_gpu_instance_times(const paradmm_gpu *h, double *begin_ms, double *end_ms)
+{
+    ok_status();
+    if (!h || !h->pk || !begin_ms || !end_ms) return pdm_set_error(PARADMM_EINVAL, "needs a packing handle");
+    const PkHost &P = *h->pk;
+    if (P.schedule != PARADMM_SCHEDULE_INSTANCE) return pdm_set_error(PARADMM_EINVAL, "instance times need the per-instance schedule");
+    unsigned long long t0 = ~0ull;
+    for (const PkStatus &s : P.status) if (s.t_begin_ns && s.t_begin_ns < t0) t0 = s.t_begin_ns;
+    for (int i = 0; i < P.n_inst; ++i) {
+        begin_ms[i] = P.status[i].t_begin_ns ? (double)(P.status[i].t_begin_ns - t0) * 1e-6 : NAN;
+        end_ms[i] = P.status[i].t_end_ns ? (double)(P.status[i].t_end_ns - t0) * 1e-6 : NAN;
+    }
+    return PARADMM_OK;
+}
+
 extern "C" int paradmm_gpu_set_profiling(paradmm_gpu *h, int on)
 {
     ok_status();
@@ -1310,7 +1341,7 @@ extern "C" void paradmm_gpu_destroy(paradmm_gpu *h)
 // paradmm.h sweep functions (GPU-backed drop-ins)
 // ===========================================================================
 static std::mutex g_sweep_mu;
-static paradmm_gpu_opts g_sweep_opts = {0, PARADMM_ENGINE_AUTO, 0, 0, 1, PARADMM_SCHEDULE_AUTO, {0}};
+static paradmm_gpu_opts g_sweep_opts = {0, PARADMM_ENGINE_AUTO, 0, 0, 1, PARADMM_SCHEDULE_AUTO, 0, {0}};
 
 struct Cached {
     paradmm_gpu *h = nullptr;

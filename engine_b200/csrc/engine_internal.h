@@ -53,6 +53,9 @@ struct PkHost {
     std::vector<long long> iters_last_call;
     int schedule = PARADMM_SCHEDULE_GRID;  // resolved schedule
     int inst_grid = 0;               // CTAs of the per-instance schedule
+    int cluster = 1;                 // CTAs per large instance in the per-instance schedule
+    int coop_min_n = 0;              // instances with N >= this are solved by a whole cluster
+    int n_coop = 0;                  // how many instances that is (the first n_coop of the order)
     int *d_order = nullptr;          // instances, largest first (per-instance schedule)
     int prof = 0;                    // per-phase timing requested
     double phase_us[4] = {0, 0, 0, 0};  // last call: mean block time per sweep (us)

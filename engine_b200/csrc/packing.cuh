@@ -84,6 +84,7 @@ struct PkStatus {
     int nonfinite;
     int nmode;              // X slots hold N (state uploaded from a graph) for the first sweep
     int pad;
+    unsigned long long t_begin_ns, t_end_ns;  // per-instance schedule: device clock at start / stop
 };
 
 // Device pointers of a packing handle (passed by value to kernels).

@@ -73,7 +73,8 @@ typedef struct paradmm_gpu_opts {
     int ctas_per_sm;  /* packing engine: resident CTAs per SM; 0 = tuned       */
     int check_every;  /* sweeps between residual-based stopping checks; 0 = 1  */
     int schedule;     /* packing engine: PARADMM_SCHEDULE_*                      */
-    int reserved[7];
+    int cluster_size; /* per-instance schedule: CTAs per large instance (1, 2, 4, 8); 0 = tuned */
+    int reserved[6];  /* reserved[0]: per-instance schedule, smallest N solved by a whole cluster (0 = 200) */
 } paradmm_gpu_opts;
 
 /* How the packing engine spreads a handle's instances over the GPU. */
@@ -178,6 +179,10 @@ int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double *circles, 
 
 /* Device memory the handle holds, in bytes. */
 int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h);
+
+/* Per-instance schedule: device-clock start and stop of every instance in
+ * the last solve/iterate call, in ms from the earliest start. */
+int paradmm_gpu_instance_times(const paradmm_gpu *h, double *begin_ms, double *end_ms);
 
 /* Kernels the handle has launched so far. */
 int64_t paradmm_gpu_launches(const paradmm_gpu *h);
