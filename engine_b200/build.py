@@ -31,6 +31,7 @@ CU_SOURCES = {
     "packing_kernels.cu": [],
     "generic_kernels.cu": ["-fmad=false"],
     "noalloc.cu": [],
+    "setmlp.cu": [],
 }
 C_SOURCES = {"graph.c": ["-O2", "-std=gnu11", "-fPIC", "-ffp-contract=off"]}
 

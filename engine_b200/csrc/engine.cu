@@ -20,6 +20,7 @@
 #include "packing_launch.h"
 #include "paradmm.h"
 #include "paradmm_gpu.h"
+#include "paradmm_learned.h"
 
 // ===========================================================================
 // Errors
@@ -1323,6 +1324,27 @@ extern "C" int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double
     int rc = pk_init_instance_state(h, instance, d_du);
     if (d_du) cudaFree(d_du);
     return rc;
+}
+
+extern "C" int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles, int radius_duals)
+{
+    ok_status();
+    if (!h || !circles) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
+    PkHost &P = *h->pk;
+    DevGuard guard(h->device);
+    std::vector<double4> z(P.n_circ);
+    for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(circles[3 * g], circles[3 * g + 1], circles[3 * g + 2], 0.0);
+    PDM_CUDA(cudaMemcpyAsync(P.D.Z, z.data(), sizeof(double4) * P.n_circ, cudaMemcpyHostToDevice, h->stream));
+    for (int i = 0; i < P.n_inst; ++i) {
+        const int grid = std::max(1, std::min(h->num_sms * 4, (int)((long long)P.inst[i].nb * (P.inst[i].nb + 1) / 2 * P.BW * P.BW / 256) + 1));
+        cudaError_t e = pk_launch_init(P.V, P.D, i, nullptr, grid, h->stream, radius_duals);
+        if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
+        P.nmode[i] = 0;
+        P.upload_iter[i] = P.it_next;
+    }
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    return PARADMM_OK;
 }
 
 extern "C" void paradmm_gpu_destroy(paradmm_gpu *h)

@@ -1,0 +1,99 @@
+"""The learned warm start: feature kernel, set-MLP gradients against the CPU
+FP64 reference, training, and the warm-start path into the packing engine."""
+import numpy as np
+import pytest
+
+import setmlp_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_set(seed=0, n=8):
+    from engine_b200 import learned
+    inst = learned.make_instances(n, seed, nmin=4, nmax=40)
+    return inst
+
+
+def test_features_match_reference():
+    from engine_b200 import learned
+    inst = _small_set(1)
+    net = learned.SetMLP(seed=3)
+    net.set_data(inst)
+    rows = sum(d["n_circles"] for d in inst)
+    f_dev = net.features(rows)
+    f_ref = setmlp_ref.features([(d["n_circles"], d["aspect"], 1.0, d["init"]) for d in inst])
+    assert np.max(np.abs(f_dev - f_ref)) < 2e-4
+    net.close()
+
+
+@pytest.mark.parametrize("seed", [2, 5])
+def test_gradients_match_fp64_reference(seed):
+    from engine_b200 import learned
+    inst = _small_set(seed)
+    rng = np.random.default_rng(seed)
+    targets = [np.stack([d["init"][:, 0] + rng.normal(0, 0.02, d["n_circles"]),
+                         d["init"][:, 1] + rng.normal(0, 0.02, d["n_circles"]),
+                         rng.uniform(0.01, 0.08, d["n_circles"])], 1) for d in inst]
+    net = learned.SetMLP(seed=seed)
+    net.set_data(inst, targets)
+    g_dev, l_dev = net.gradients(0, len(inst))
+    rows = sum(d["n_circles"] for d in inst)
+    F = net.features(rows)
+    sizes = [d["n_circles"] for d in inst]
+    T = np.zeros((rows, 4))
+    r0 = 0
+    for d, t in zip(inst, targets):
+        s = np.sqrt(d["aspect"] / d["n_circles"])
+        n = d["n_circles"]
+        T[r0:r0 + n, 0] = (t[:, 0] - d["init"][:, 0]) / s
+        T[r0:r0 + n, 1] = (t[:, 1] - d["init"][:, 1]) / s
+        T[r0:r0 + n, 2] = t[:, 2] / s
+        r0 += n
+    l_ref, g_ref = setmlp_ref.loss_and_grads(net.params(), F, T, sizes)
+    assert abs(l_dev - l_ref) <= 1e-4 * abs(l_ref)
+    off = 0
+    for name, cnt in (("W1", 128 * 32), ("b1", 128), ("W2", 128 * 256), ("b2", 128), ("W3", 4 * 128), ("b3", 4)):
+        a, b = g_dev[off:off + cnt], g_ref[off:off + cnt]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        assert rel < 2e-3, f"{name}: relative error {rel:.2e}"
+        off += cnt
+    net.close()
+
+
+def test_training_reduces_loss():
+    from engine_b200 import learned
+    inst = learned.make_instances(64, 11, nmin=10, nmax=60)
+    # a smooth synthetic target: each circle moves toward the box centre and
+    # takes a radius set by its nearest-neighbour distance
+    targets = []
+    for d in inst:
+        c = d["init"]
+        dd = np.sqrt(((c[:, None, :2] - c[None, :, :2]) ** 2).sum(-1)) + np.eye(len(c)) * 9
+        tgt = np.stack([c[:, 0] + 0.1 * (d["aspect"] / 2 - c[:, 0]), c[:, 1] + 0.1 * (0.5 - c[:, 1]),
+                        0.45 * dd.min(1)], 1)
+        targets.append(tgt)
+    net = learned.SetMLP(seed=1)
+    net.set_data(inst, targets)
+    l0 = net.eval()
+    losses = net.train(epochs=60, batch_inst=16, lr=2e-3, lr_end=2e-4)
+    l1 = net.eval()
+    assert l1 < 0.2 * l0, (l0, l1, losses[-5:])
+    net.close()
+
+
+def test_warm_start_from_converged_packing_converges_fast():
+    """The warm-start path itself: starting from a converged packing (the
+    best possible proposal) converges in far fewer sweeps than the plain
+    start, and from a noisy copy of it the residual still decides."""
+    from engine_b200 import learned
+    inst = learned.make_instances(6, 21, nmin=30, nmax=80)
+    plain = learned.solve_plain(inst)
+    its_plain = [s["iterations"] for s in plain["stats"]]
+    b = learned.Batch(inst)
+    b.warm_start(np.concatenate(plain["circles"]), radius_duals=1)
+    b.solve(20000, 1e-5)
+    st = b.stats()
+    assert all(s["converged"] for s in st)
+    its_warm = [s["iterations"] for s in st]
+    assert sum(its_warm) < 0.5 * sum(its_plain), (its_warm, its_plain)
+    b.close()
