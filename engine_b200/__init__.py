@@ -142,6 +142,8 @@ _SIGS = {
     "paradmm_gpu_launches": (C.c_int64, [C.c_void_p]),
     "paradmm_gpu_instance_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "paradmm_gpu_set_fallback": (C.c_int, [C.c_void_p, C.c_int64]),
+    "paradmm_gpu_instance_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "paradmm_gpu_pin_graph": (C.c_int, [C.POINTER(Graph)]),
     "paradmm_gpu_unpin_graph": (C.c_int, [C.POINTER(Graph)]),
@@ -417,6 +419,17 @@ class Handle:
 
     def set_profiling(self, on: bool) -> None:
         check(self.lib.paradmm_gpu_set_profiling(self.ptr, 1 if on else 0))
+
+    def set_fallback(self, after_sweeps: int) -> None:
+        """Per-instance schedule: restart unconverged instances from their plain
+        start after this many sweeps of a solve call (0: off)."""
+        check(self.lib.paradmm_gpu_set_fallback(self.ptr, int(after_sweeps)))
+
+    def instance_fallbacks(self) -> np.ndarray:
+        """1 for every instance that fell back to its plain start in the last call."""
+        out = np.zeros(self.instances(), dtype=np.int32)
+        check(self.lib.paradmm_gpu_instance_fallbacks(self.ptr, out.ctypes.data_as(C.POINTER(C.c_int))))
+        return out
 
     def phase_times(self) -> list[float]:
         """Mean block time per sweep (us): pass, barrier 1, finalise, barrier 2."""

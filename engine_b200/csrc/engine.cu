@@ -407,6 +407,7 @@ static int pk_finalize_build(paradmm_gpu *h)
         std::vector<double4> z(P.n_circ);
         for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(P.init_Z[3 * g], P.init_Z[3 * g + 1], P.init_Z[3 * g + 2], 0.0);
         if ((rc = dput(h, &D.Z, z))) return rc;
+        if ((rc = dput(h, (double4 **)&D.Z0, z))) return rc;
     }
     if ((rc = dalloc(h, (void **)&D.local_part, sizeof(double4) * (size_t)P.n_circ))) return rc;
     if ((rc = dput(h, (int2 **)&D.fin_items, fin))) return rc;
@@ -757,6 +758,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
         s.converged = 0;
         s.nonfinite = 0;
         s.nmode = P.nmode[i];
+        s.pad = 0;
         s.t_begin_ns = s.t_end_ns = 0;
     }
     PDM_CUDA(cudaMemcpyAsync(P.D.status, st.data(), sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
@@ -768,6 +770,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     R.dynamic = 0;
     R.tol = tol;
     R.check_every = check_every < 1 ? 1 : check_every;
+    R.fallback_after = P.fallback_after < n ? P.fallback_after : 0;
     PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
     cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, &h->ctl->item_ctr[0],
                                         P.inst_grid, P.cluster, h->stream);
@@ -1336,14 +1339,40 @@ extern "C" int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles,
     std::vector<double4> z(P.n_circ);
     for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(circles[3 * g], circles[3 * g + 1], circles[3 * g + 2], 0.0);
     PDM_CUDA(cudaMemcpyAsync(P.D.Z, z.data(), sizeof(double4) * P.n_circ, cudaMemcpyHostToDevice, h->stream));
+    // one launch over all instances (grid.y = instance) when the grid allows it
+    long long slots = 0;
+    for (int i = 0; i < P.n_inst; ++i) slots = std::max(slots, (long long)P.inst[i].nb * (P.inst[i].nb + 1) / 2 * P.BW * P.BW);
+    const int grid = (int)std::max(1LL, std::min<long long>(h->num_sms * 4, slots / 256 + 1));
     for (int i = 0; i < P.n_inst; ++i) {
-        const int grid = std::max(1, std::min(h->num_sms * 4, (int)((long long)P.inst[i].nb * (P.inst[i].nb + 1) / 2 * P.BW * P.BW / 256) + 1));
-        cudaError_t e = pk_launch_init(P.V, P.D, i, nullptr, grid, h->stream, radius_duals);
-        if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
+        if (P.n_inst > 65535 || i == 0) {
+            cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, nullptr, grid, h->stream, radius_duals);
+            if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
+        }
         P.nmode[i] = 0;
         P.upload_iter[i] = P.it_next;
     }
     PDM_CUDA(cudaStreamSynchronize(h->stream));
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps)
+{
+    ok_status();
+    if (!h) return pdm_set_error(PARADMM_EINVAL, "handle is NULL");
+    if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
+    if (after_sweeps < 0 || after_sweeps > INT_MAX) return pdm_set_error(PARADMM_EINVAL, "after_sweeps out of range");
+    if (after_sweeps > 0 && h->pk->schedule != PARADMM_SCHEDULE_INSTANCE)
+        return pdm_set_error(PARADMM_EINVAL, "the in-call fallback needs the per-instance schedule");
+    h->pk->fallback_after = (int)after_sweeps;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_instance_fallbacks(const paradmm_gpu *h, int *restarted)
+{
+    ok_status();
+    if (!h || !restarted) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
+    for (int i = 0; i < h->pk->n_inst; ++i) restarted[i] = h->pk->status[i].pad != 0;
     return PARADMM_OK;
 }
 

@@ -58,6 +58,7 @@ struct PkHost {
     int n_coop = 0;                  // how many instances that is (the first n_coop of the order)
     int *d_order = nullptr;          // instances, largest first (per-instance schedule)
     int prof = 0;                    // per-phase timing requested
+    int fallback_after = 0;          // per-instance schedule: restart from the plain start after this many sweeps
     double phase_us[4] = {0, 0, 0, 0};  // last call: mean block time per sweep (us)
     // reference-layout maps (graph handles)
     int2 *d_pmap = nullptr; long long n_pmap = 0;

@@ -98,6 +98,7 @@ struct PkDev {
     double4 *row_part;       // [tile][BW] sums of M over the row circle's pair edges
     double4 *col_part;       // [tile][BW] same for the column circle
     double4 *Z;              // [circle] consensus (cx, cy, r, -)
+    const double4 *Z0;       // [circle] the instance's plain start (fallback target)
     double4 *local_part;     // [circle] rho-weighted wall + radius contributions
     const int2 *fin_items;   // [n_fin] consensus items (instance, circle block)
     int n_fin, pad2;
@@ -125,6 +126,8 @@ struct PkRun {
     double tol;       // stop when primal + dual <= tol (tol < 0: never)
     int check_every;  // sweeps between stopping checks
     int prof;         // accumulate per-phase block times into DevCtl::prof
+    int fallback_after;  // per-instance schedule: restart an unconverged instance from Z0 after this many sweeps (0: never)
+    int pad2;
 };
 
 PDM_HD long long pk_tri(int I, int J, int nb) { return (long long)I * nb - (long long)I * (I - 1) / 2 + (J - I); }

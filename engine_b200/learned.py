@@ -10,9 +10,9 @@ plain ADMM converges to.
 
 solve_plain / solve_learned time both paths on the same instances:
   plain    create the batch handle (plain start) [untimed], then solve;
-  learned  features + network forward + warm start + solve with a budget,
-           then the instances that did not converge are re-solved from the
-           plain start (fallback); the residual decides.
+  learned  features + network forward + warm start + one solve in which an
+           instance not converged within the budget restarts from its plain
+           start inside the same launch (fallback); the residual decides.
 Times are host wall clock around the calls (device work included).
 """
 from __future__ import annotations
@@ -96,12 +96,13 @@ def _descs(instances):
 class Batch:
     """A packing handle over a list of instances (plain start)."""
 
-    def __init__(self, instances, device=0, schedule=0, cluster=0):
+    def __init__(self, instances, device=0, schedule=0, cluster=0, coop_min_n=0):
         from . import opts
         self.lib = load()
         self.instances = instances
         arr, self._keep = _descs(instances)
         o = opts(device=device, schedule=schedule, cluster_size=cluster)
+        o.reserved[0] = coop_min_n
         p = C.c_void_p()
         check(self.lib.paradmm_gpu_create_packing(arr, len(instances), C.byref(o), C.byref(p)))
         self.h = p
@@ -125,6 +126,14 @@ class Batch:
             c = np.zeros((d["n_circles"], 3))
             check(self.lib.paradmm_gpu_get_circles(self.h, i, c.ctypes.data_as(_P)))
             out.append(c)
+        return out
+
+    def set_fallback(self, after_sweeps: int) -> None:
+        check(self.lib.paradmm_gpu_set_fallback(self.h, int(after_sweeps)))
+
+    def fallbacks(self) -> np.ndarray:
+        out = np.zeros(len(self.instances), dtype=np.int32)
+        check(self.lib.paradmm_gpu_instance_fallbacks(self.h, out.ctypes.data_as(C.POINTER(C.c_int))))
         return out
 
     def warm_start(self, circles: np.ndarray, radius_duals: int = 1) -> None:
@@ -253,27 +262,21 @@ def solve_plain(instances, maxiter=20000, tol=1e-5, device=0):
 
 
 def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, radius_duals=1, device=0):
+    """Learned path: network proposal -> warm start -> one solve in which every
+    instance still unconverged after `budget` sweeps restarts from its plain
+    start (in the same launch) and gets the plain path's full maxiter."""
     b = Batch(instances, device=device)
     t = time.perf_counter()
     net.set_data(instances)
     prop = net.predict()
     b.warm_start(prop, radius_duals)
-    s = b.solve(budget, tol)
-    st = b.stats()
-    fail = [i for i, x in enumerate(st) if not x["converged"]]
-    circ = b.circles()
-    fb = None
-    if fail:
-        fb_inst = [instances[i] for i in fail]
-        bf = Batch(fb_inst, device=device)
-        bf.solve(maxiter, tol)
-        fst = bf.stats()
-        fc = bf.circles()
-        bf.close()
-        for j, i in enumerate(fail):
-            st[i] = dict(fst[j], fallback=1)
-            circ[i] = fc[j]
-        fb = len(fail)
+    b.set_fallback(budget)
+    s = b.solve(budget + maxiter, tol)
     wall = time.perf_counter() - t
+    st = b.stats()
+    fb = b.fallbacks()
+    for i, x in enumerate(st):
+        x["fallback"] = int(fb[i])
+    circ = b.circles()
     b.close()
-    return dict(wall_s=wall, device_ms=s["device_ms"], stats=st, circles=circ, fallbacks=fb or 0, proposal=prop)
+    return dict(wall_s=wall, device_ms=s["device_ms"], stats=st, circles=circ, fallbacks=int(fb.sum()), proposal=prop)

@@ -177,6 +177,19 @@ int paradmm_gpu_get_circles(paradmm_gpu *h, int instance, double *out);
  * [u_cx_i, u_cy_i, u_r_i, u_cx_j, u_cy_j, u_r_j]. */
 int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double *circles, const float *pair_duals);
 
+/* In-call fallback for warm starts (per-instance schedule only; no reference
+ * counterpart).  With after_sweeps > 0, every later paradmm_gpu_solve call
+ * restarts an instance that has not converged after after_sweeps sweeps of
+ * that call (or whose residual became NaN/Inf before then) from its plain
+ * start -- the circles given at creation, X = Z on every edge, every dual 0 --
+ * and continues it for the rest of the call's maxiter, inside the same
+ * launch.  0 (the default) switches it off.  EINVAL on a grid-schedule handle. */
+int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps);
+
+/* restarted[i] = 1 if instance i fell back to its plain start in the last
+ * solve call, else 0. */
+int paradmm_gpu_instance_fallbacks(const paradmm_gpu *h, int *restarted);
+
 /* Device memory the handle holds, in bytes. */
 int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h);
 

@@ -97,3 +97,49 @@ def test_warm_start_from_converged_packing_converges_fast():
     its_warm = [s["iterations"] for s in st]
     assert sum(its_warm) < 0.5 * sum(its_plain), (its_warm, its_plain)
     b.close()
+
+
+@pytest.mark.parametrize("cluster", [1, 2])
+def test_in_call_fallback_equals_plain_solve(cluster):
+    """An instance whose warm start does not converge within the budget
+    restarts from its plain start inside the same launch: from there on its
+    trajectory is the plain solve's, so it ends on the plain solve's circles
+    bit for bit after budget + (plain sweeps) sweeps.  Sizes cover the
+    on-chip small-instance path (N <= 40), the tiled one-CTA path and the
+    cluster path (N >= 60 here)."""
+    from engine_b200 import SCHEDULE_INSTANCE, learned
+    inst = learned.make_instances(12, 31, nmin=12, nmax=110)
+    budget = 25
+    kw = dict(schedule=SCHEDULE_INSTANCE, cluster=cluster, coop_min_n=60)
+    bp = learned.Batch(inst, **kw)
+    bp.solve(20000, 1e-5)
+    st_p, circ_p = bp.stats(), bp.circles()
+    bp.close()
+    rng = np.random.default_rng(5)
+    prop = np.concatenate([d["init"] + rng.normal(0, 0.05, d["init"].shape) * [1, 1, 0.1] for d in inst])
+    prop[:, 2] = np.abs(prop[:, 2])
+    b = learned.Batch(inst, **kw)
+    b.warm_start(prop, radius_duals=1)
+    b.set_fallback(budget)
+    b.solve(budget + 20000, 1e-5)
+    st, circ, fb = b.stats(), b.circles(), b.fallbacks()
+    b.close()
+    assert fb.sum() > 0
+    for i in range(len(inst)):
+        if not fb[i]:
+            assert st[i]["converged"] and st[i]["iterations"] <= budget
+            continue
+        assert st[i]["iterations"] == budget + st_p[i]["iterations"], (i, st[i]["iterations"], st_p[i]["iterations"])
+        assert st[i]["converged"] == st_p[i]["converged"]
+        assert np.array_equal(circ[i], circ_p[i]), i
+
+
+def test_fallback_needs_instance_schedule():
+    from engine_b200 import SCHEDULE_GRID, learned
+    from engine_b200 import ParadmmError
+    inst = learned.make_instances(2, 3, nmin=10, nmax=20)
+    b = learned.Batch(inst, schedule=SCHEDULE_GRID)
+    with pytest.raises(ParadmmError):
+        b.set_fallback(10)
+    b.set_fallback(0)
+    b.close()
