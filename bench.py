@@ -6,8 +6,9 @@ Workload (one "step" = one full sweep X/M/Z/U/N of the factor graph):
   factors, 32,000 wall factors, 8,000 radius factors, 128,056,000 edges;
   seeded uniform init (centres in the box, radii in [0, 0.01]), rho = 10,
   rho on radius-factor edges = 5, alpha = 1, radius exponent 2.  The FP32
-  edge state is 1.55 GB, larger than the 126 MB L2, so no L2 flush is needed
-  between steps.
+  edge state (U of the pair edges; X and U of wall and radius edges) is
+  0.77 GB, larger than the 126 MB L2, so no L2 flush is needed between
+  steps.
 
 Arms:
   default           the engine (libparadmm_b200.so).  `value` is device-timed
@@ -50,9 +51,11 @@ def edges_of(n: int) -> int:
 
 
 def algo_bytes_per_sweep(n: int) -> int:
-    """16 B per live FP32 component (X and U, each read and written):
-    pair 6 components, wall 3, radius 1."""
-    return (n * (n - 1) // 2) * 96 + N_WALLS * n * 48 + n * 16
+    """Bytes one sweep must move: pair edges keep only U (X is recomputed
+    from the previous consensus and U), so 8 B per live component (U read and
+    written), 6 components; wall and radius edges keep X and U, 16 B per
+    component (3 and 1 components)."""
+    return (n * (n - 1) // 2) * 48 + N_WALLS * n * 48 + n * 16
 
 
 def measured_peak():
@@ -65,7 +68,7 @@ def measured_peak():
 
 def profiled_traffic():
     """DRAM bytes per sweep from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "packing_sweep_n8000.md")
+    p = os.path.join(ROOT, "profiles", "pk_persistent_n4000_full.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -309,6 +312,8 @@ def run_engine_arm(args):
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": None if traffic_sweep is None else traffic_sweep * sweeps_per_launch,
                          "algorithmic_bytes_per_sweep": algo, "sweeps_per_launch": sweeps_per_launch,
+                         "algorithmic_bytes": "48 B per pair factor (U of 6 live components, read + written; "
+                                              "X recomputed), 48 B per wall factor, 16 B per radius factor",
                          "kernel": "pk_persistent"},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -408,6 +408,9 @@ static int pk_finalize_build(paradmm_gpu *h)
         for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(P.init_Z[3 * g], P.init_Z[3 * g + 1], P.init_Z[3 * g + 2], 0.0);
         if ((rc = dput(h, &D.Z, z))) return rc;
         if ((rc = dput(h, (double4 **)&D.Z0, z))) return rc;
+        std::vector<float4> zp(P.n_circ);
+        for (int g = 0; g < P.n_circ; ++g) zp[g] = make_float4((float)z[g].x, (float)z[g].y, (float)z[g].z, 0.f);
+        if ((rc = dput(h, &D.Zp, zp))) return rc;
     }
     if ((rc = dalloc(h, (void **)&D.local_part, sizeof(double4) * (size_t)P.n_circ))) return rc;
     if ((rc = dput(h, (int2 **)&D.fin_items, fin))) return rc;
@@ -477,7 +480,7 @@ static int pk_finalize_build(paradmm_gpu *h)
             for (int q = 0; q < P.n_inst && P.inst[order[q]].N >= P.coop_min_n; ++q) P.n_coop = q + 1;
     }
     P.upload_iter.assign(P.n_inst, 0);
-    P.nmode.assign(P.n_inst, 0);
+    P.nmode.assign(P.n_inst, PK_MODE_Z);
     P.status.assign(P.n_inst, PkStatus{});
     for (auto &s : P.status) { s.resid_iter = -1; s.primal = s.dual = NAN; }
     P.iters_last_call.assign(P.n_inst, 0);
@@ -490,7 +493,7 @@ static int pk_init_instance_state(paradmm_gpu *h, int inst, const float *d_pair_
     cudaError_t e = pk_launch_init(P.V, P.D, inst, d_pair_duals, h->num_sms * 4, h->stream);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
     PDM_CUDA(cudaStreamSynchronize(h->stream));
-    P.nmode[inst] = 0;
+    P.nmode[inst] = PK_MODE_Z;
     P.upload_iter[inst] = P.it_next;
     return PARADMM_OK;
 }
@@ -700,6 +703,7 @@ static int pk_upload_graph(paradmm_gpu *h, const graph *G)
     PkHost &P = *h->pk;
     int rc = ensure_stage(h);
     if (rc) return rc;
+    if (!P.D.aux && (rc = dalloc(h, (void **)&P.D.aux, (size_t)(P.n_tiles * pk_tile_floats(P.BW) * 4LL)))) return rc;
     const size_t ne = (size_t)h->num_edges * 2, nz = (size_t)h->num_vars * 2;
     PDM_CUDA(cudaMemcpyAsync(h->d_stage[2], G->N, sizeof(double) * ne, cudaMemcpyHostToDevice, h->stream));
     PDM_CUDA(cudaMemcpyAsync(h->d_stage[3], G->U, sizeof(double) * ne, cudaMemcpyHostToDevice, h->stream));
@@ -716,7 +720,7 @@ static int pk_upload_graph(paradmm_gpu *h, const graph *G)
         return pdm_set_error(PARADMM_EUNSUPPORTED_GRAPH,
                              "the uploaded state has radius edges whose two components differ; "
                              "the packing engine keeps one (use PARADMM_ENGINE_GENERIC_F64)");
-    P.nmode[0] = 1;
+    P.nmode[0] = PK_MODE_N;
     P.upload_iter[0] = P.it_next;
     return PARADMM_OK;
 }
@@ -734,11 +738,20 @@ static int pk_download_graph(paradmm_gpu *h, graph *G)
     const size_t ne = (size_t)h->num_edges * 2, nz = (size_t)h->num_vars * 2;
     double *dst[5] = {G->X, G->M, G->N, G->U, G->Z};
     for (int q = 0; q < 5; ++q) {
-        if (nm && q < 2) continue;  // no sweep since the upload: X and M are the caller's
+        if (nm == PK_MODE_N && q < 2) continue;  // no sweep since the upload: X and M are the caller's
         PDM_CUDA(cudaMemcpyAsync(dst[q], h->d_stage[q], sizeof(double) * (q == 4 ? nz : ne), cudaMemcpyDeviceToHost, h->stream));
     }
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     return PARADMM_OK;
+}
+
+// The first-sweep mode an instance still owes its next sweep after a launch
+// in which `last` was its last executed sweep (PK_MODE_RECOMPUTE: none).
+static int pk_pending_mode(const PkStatus &s, long long last)
+{
+    if (last < s.mode_iter) return s.nmode;                         // the mode's sweep did not run
+    if (last == s.mode_iter && s.nmode == PK_MODE_N) return PK_MODE_XN;  // X of that sweep came from N
+    return PK_MODE_RECOMPUTE;
 }
 
 // Runs up to n sweeps of every instance (persistent launches of at most
@@ -758,6 +771,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
         s.converged = 0;
         s.nonfinite = 0;
         s.nmode = P.nmode[i];
+        s.mode_iter = it0;
         s.pad = 0;
         s.t_begin_ns = s.t_end_ns = 0;
     }
@@ -786,7 +800,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     for (int i = 0; i < P.n_inst; ++i) {
         const long long ran = st[i].last_iter - it0 + 1;
         P.iters_last_call[i] = ran > 0 ? ran : 0;
-        if (ran > 0) P.nmode[i] = 0;
+        P.nmode[i] = pk_pending_mode(st[i], st[i].last_iter);
         P.status[i] = st[i];
         if (st[i].nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
     }
@@ -816,6 +830,7 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
             s.converged = 0;
             s.nonfinite = 0;
             s.nmode = P.nmode[i];
+            s.mode_iter = it0;
             if (!done[i]) ++active;
         }
         if (active == 0) break;
@@ -850,7 +865,8 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
             if (done[i]) continue;
             const long long last = std::min(st[i].last_iter, it0 + sweeps - 1);
             const long long ran = last - it0 + 1;
-            if (ran > 0) { P.iters_last_call[i] += ran; P.nmode[i] = 0; }
+            if (ran > 0) P.iters_last_call[i] += ran;
+            P.nmode[i] = pk_pending_mode(st[i], last);
             P.status[i] = st[i];
             if (st[i].converged || st[i].nonfinite) done[i] = 1;
             if (st[i].nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
@@ -1348,7 +1364,7 @@ extern "C" int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles,
             cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, nullptr, grid, h->stream, radius_duals);
             if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
         }
-        P.nmode[i] = 0;
+        P.nmode[i] = PK_MODE_Z;
         P.upload_iter[i] = P.it_next;
     }
     PDM_CUDA(cudaStreamSynchronize(h->stream));

@@ -91,7 +91,7 @@ extern "C" int64_t paradmm_noalloc_state_bytes(int n_circles, int n_walls)
 {
     if (n_circles < 2 || n_circles > NA_MAX_CIRCLES || n_walls < 0 || n_walls > NA_MAX_WALLS) return -1;
     return na_tiles_of(n_circles) * pk_tile_floats(NA_BW) * 4 + (int64_t)n_circles * n_walls * 2 * sizeof(float4) +
-           (int64_t)n_circles * sizeof(float2);
+           (int64_t)n_circles * sizeof(float2) + (int64_t)n_circles * sizeof(float4) + 16;
 }
 
 // Per-device set-up: the scratch's device address (cudaGetSymbolAddress with
@@ -224,13 +224,17 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     D.rad_coef = (const float4 *)(base + NaLayout::rad_coef);
     D.rad_rho = (const double *)(base + NaLayout::rad_rho);
     D.ctl = (DevCtl *)(base + NaLayout::ctl);
-    // caller-owned edge state: pair tiles, then wall X, wall U, radius (X, U)
+    // caller-owned edge state: pair tiles (U), wall X, wall U, radius (X, U),
+    // the previous sweep's circles (FP32) and a 16-byte header holding the
+    // first-sweep mode the state owes its next sweep
     const int64_t tile_bytes = na_tiles_of(N) * pk_tile_floats(NA_BW) * 4;
     const int nwall = N * d.n_walls;
     D.tiles = (float *)d_state;
     D.wall_X = (float4 *)((char *)d_state + tile_bytes);
     D.wall_U = D.wall_X + nwall;
     D.rad_XU = (float2 *)(D.wall_U + nwall);
+    D.Zp = (float4 *)(D.rad_XU + N);
+    int *d_mode = (int *)(D.Zp + N);
 
     // Tables into the scratch; residual partials start at zero (the array
     // keeps whatever the previous call left).
@@ -252,9 +256,16 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     // consensus: caller's [cx, cy, r] rows -> the kernel's (cx, cy, r, -) rows
     PDM_CUDA(cudaMemcpy2DAsync(D.Z, sizeof(double4), d_circles, 3 * sizeof(double), 3 * sizeof(double), N,
                                cudaMemcpyDeviceToDevice, s));
+    static int s_mode;
     if (init_state) {
         cudaError_t e = pk_launch_init(NA_V, D, 0, nullptr, g_na_grid[device], s);
         if (e != cudaSuccess) return pdm_cuda_fail(e, "noalloc init", __FILE__, __LINE__);
+        s_mode = PK_MODE_Z;
+    } else {
+        PDM_CUDA(cudaMemcpyAsync(&s_mode, d_mode, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PDM_CUDA(cudaStreamSynchronize(s));
+        if (s_mode < PK_MODE_RECOMPUTE || s_mode > PK_MODE_XN)
+            return pdm_set_error(PARADMM_EINVAL, "noalloc: the state buffer was never initialised (call with init_state = 1)");
     }
 
     const auto t0 = std::chrono::steady_clock::now();
@@ -269,6 +280,8 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         s_status.check_from = it0 + 2;
         s_status.resid_iter = -1;
         s_status.primal = s_status.dual = NAN;
+        s_status.nmode = s_mode;
+        s_status.mode_iter = it0;
         memset(&s_ctl, 0, sizeof s_ctl);
         s_ctl.n_active = 1;
         PDM_CUDA(cudaMemcpyAsync(D.status, &s_status, sizeof s_status, cudaMemcpyHostToDevice, s));
@@ -287,16 +300,21 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         PDM_CUDA(cudaStreamSynchronize(s));
         if (s_ctl.err != DEV_OK)
             return pdm_set_error(PARADMM_ETIMEOUT, "noalloc: a grid barrier wait ran out (device error %d)", s_ctl.err);
-        const long long ran = std::min<long long>(s_status.last_iter, it0 + s_ctl.pad[0] - 1) - it0 + 1;
+        const long long last = std::min<long long>(s_status.last_iter, it0 + s_ctl.pad[0] - 1);
+        const long long ran = last - it0 + 1;
         done += ran;
+        if (last < s_status.mode_iter) s_mode = s_status.nmode;
+        else if (last == s_status.mode_iter && s_status.nmode == PK_MODE_N) s_mode = PK_MODE_XN;
+        else s_mode = PK_MODE_RECOMPUTE;
         it0 += s_ctl.pad[0];
         left -= s_ctl.pad[0];
         if (s_status.nonfinite) { status_rc = pdm_set_error(PARADMM_ENONFINITE, "noalloc: residual became NaN/Inf"); break; }
         if (s_status.converged || (long long)s_ctl.pad[0] < chunk) break;
     }
-    // consensus back to the caller's rows
+    // consensus back to the caller's rows; the mode into the state header
     PDM_CUDA(cudaMemcpy2DAsync(d_circles, 3 * sizeof(double), D.Z, sizeof(double4), 3 * sizeof(double), N,
                                cudaMemcpyDeviceToDevice, s));
+    PDM_CUDA(cudaMemcpyAsync(d_mode, &s_mode, sizeof(int), cudaMemcpyHostToDevice, s));
     PDM_CUDA(cudaStreamSynchronize(s));
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (stats) {

@@ -12,25 +12,38 @@
 //
 // One ADMM sweep (reference core/paradmm.c:736-741: updateXM, updateZ,
 // updateUN) is restated as ONE pass over the edge state plus a consensus
-// finalisation.  The state kept per live edge component is X^k and U^(k-1)
-// (FP32); sweep k+1 then does, per component,
+// finalisation.  The only state kept per live pair-edge component is
+// U^(k-1) (FP32), plus, per circle, Z^k (FP64) and Zp = Z^(k-1) (FP32).
+// X^k is not stored: it is prox(Zp - U^(k-1)), recomputed with the same
+// FP32 operations that produced it in the previous pass.  Sweep k+1 then
+// does, per component,
+//     X^k = prox(Z^(k-1) - U^(k-1))          (recomputed)
 //     U^k = U^(k-1) + alpha (X^k - Z^k)      (updateU of sweep k)
 //     N^k = Z^k - U^k                        (updateN of sweep k)
 //     X^(k+1) = prox(N^k)                    (updateX of sweep k+1)
 //     M = X^(k+1) + U^k                      (updateM of sweep k+1)
 // and accumulates rho*M into per-circle FP64 partial sums, which the
 // finalisation turns into Z^(k+1) (updateZ of sweep k+1).  So each sweep
-// reads and writes X and U once: 16 bytes per live component.
+// reads and writes U once: 8 bytes per live component.  The prox of a pair
+// is a few dozen FP32 operations, far cheaper than the 24 bytes of X it
+// replaces.  The first sweep after a state change has no previous X to
+// recompute; PkStatus::nmode says what stands in for it:
+//     PK_MODE_Z  X^k = Z^k (plain or warm start: U^k = U^(k-1))
+//     PK_MODE_N  N^k and U^k given (state uploaded from a reference graph;
+//                N lives in the aux tiles); the sweep after it recomputes
+//                X from that N (PK_MODE_XN), not from Z - U
+// Wall and radius edges (a few per circle) keep X and U explicitly.
 //
 // Pair state layout.  Circles are cut into blocks of BW = 32*V; the pairs of
 // block I against block J >= I form tile (I, J), numbered row-major over the
 // upper triangle.  A tile is BW rows (circle i) x 6 components x BW columns
-// (circle j) x {X, U} floats:
-//     tile[row][comp][col][xu],   comp = cx_i, cy_i, r_i, cx_j, cy_j, r_j
-// so the 32 lanes of a warp, lane l owning columns [V l, V l + V), read and
-// write one row's component as one contiguous 256*V-byte segment (V = 2:
-// one float4 per lane holding X,U of two columns).  Diagonal tiles only use
-// col > row; slots outside the triangle or past N are never touched.
+// (circle j) of U floats.  Lane l of a warp owns columns [V l, V l + V);
+// its 6V values of a row, q = comp * V + (col - V l) with comp = cx_i, cy_i,
+// r_i, cx_j, cy_j, r_j, sit in 16-byte chunks: chunk q/4 of lane l at float
+// (q/4) * 128 + 4 l (pk_uoff).  So the warp moves a row as 3V/2 fully
+// coalesced 512-byte segments and each lane touches only its own chunks.
+// Diagonal tiles only use col > row; slots outside the triangle or past N
+// are never touched.
 #pragma once
 
 #include <stdint.h>
@@ -40,6 +53,12 @@
 #define PK_THREADS 256
 #define PK_WARPS (PK_THREADS / 32)
 #define PK_COMPS 6
+
+// First-sweep modes (PkStatus::nmode).
+#define PK_MODE_RECOMPUTE 0
+#define PK_MODE_Z 1
+#define PK_MODE_N 2
+#define PK_MODE_XN 3
 
 // Per-instance constants.
 struct PkInst {
@@ -82,8 +101,9 @@ struct PkStatus {
     double primal, dual;
     int converged;
     int nonfinite;
-    int nmode;              // X slots hold N (state uploaded from a graph) for the first sweep
-    int pad;
+    int nmode;              // PK_MODE_* of sweep mode_iter (every other sweep recomputes X)
+    int pad;                // 1 once the instance fell back to its plain start (per-instance schedule)
+    long long mode_iter;    // sweep index the mode applies to
     unsigned long long t_begin_ns, t_end_ns;  // per-instance schedule: device clock at start / stop
 };
 
@@ -99,6 +119,8 @@ struct PkDev {
     double4 *col_part;       // [tile][BW] same for the column circle
     double4 *Z;              // [circle] consensus (cx, cy, r, -)
     const double4 *Z0;       // [circle] the instance's plain start (fallback target)
+    float4 *Zp;              // [circle] Z of the previous sweep (FP32: the values the pass used)
+    float *aux;              // N of the pair edges for PK_MODE_N (tile layout; graph handles only)
     double4 *local_part;     // [circle] rho-weighted wall + radius contributions
     const int2 *fin_items;   // [n_fin] consensus items (instance, circle block)
     int n_fin, pad2;
@@ -131,4 +153,20 @@ struct PkRun {
 };
 
 PDM_HD long long pk_tri(int I, int J, int nb) { return (long long)I * nb - (long long)I * (I - 1) / 2 + (J - I); }
-PDM_HD long long pk_tile_floats(int BW) { return (long long)BW * PK_COMPS * 2 * BW; }
+PDM_HD long long pk_tile_floats(int BW) { return (long long)BW * PK_COMPS * BW; }
+
+// Mode of sweep k for an instance whose status is st.
+PDM_HD int pk_mode_at(int nmode, long long mode_iter, long long k)
+{
+    if (k == mode_iter) return nmode;
+    if (k == mode_iter + 1 && nmode == PK_MODE_N) return PK_MODE_XN;
+    return PK_MODE_RECOMPUTE;
+}
+
+// Float offset of (component, column) within a tile row (layout above).
+template <int V>
+PDM_HD int pk_uoff(int comp, int col)
+{
+    const int q = comp * V + col % V;
+    return (q >> 2) * 128 + (col / V) * 4 + (q & 3);
+}
