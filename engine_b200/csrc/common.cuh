@@ -144,6 +144,28 @@ PDM_D double warp_sum(double v)
 
 // Block-wide sum (any blockDim multiple of 32, <= 1024); result valid in all
 // threads.  Fixed reduction order, so the result is deterministic.
+// Sums two values over the block (every thread gets both sums).
+PDM_D double2 block_sum2(double a, double b)
+{
+    __shared__ double s_p[2][32];
+    __shared__ double2 s_t;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) { s_p[0][w] = a; s_p[1][w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double x = l < nw ? s_p[0][l] : 0.0, y = l < nw ? s_p[1][l] : 0.0;
+        x = warp_sum(x);
+        y = warp_sum(y);
+        if (l == 0) s_t = make_double2(x, y);
+    }
+    __syncthreads();
+    return s_t;
+}
+
 PDM_D double block_sum(double v)
 {
     __shared__ double s_part[32];

@@ -414,10 +414,8 @@ static int pk_finalize_build(paradmm_gpu *h)
     }
     if ((rc = dalloc(h, (void **)&D.local_part, sizeof(double4) * (size_t)P.n_circ))) return rc;
     if ((rc = dput(h, (int2 **)&D.fin_items, fin))) return rc;
-    if ((rc = dalloc(h, (void **)&D.item_primal, sizeof(double) * 2 * (size_t)P.n_items))) return rc;
     if ((rc = dalloc(h, (void **)&D.blk_primal, sizeof(double) * 4 * (size_t)D.n_fin))) return rc;
     if ((rc = dalloc(h, (void **)&D.blk_dual, sizeof(double) * 4 * (size_t)D.n_fin))) return rc;
-    PDM_CUDA(cudaMemset(D.item_primal, 0, sizeof(double) * 2 * (size_t)P.n_items));
     PDM_CUDA(cudaMemset(D.blk_primal, 0, sizeof(double) * 4 * (size_t)D.n_fin));
     PDM_CUDA(cudaMemset(D.blk_dual, 0, sizeof(double) * 4 * (size_t)D.n_fin));
     if ((rc = dalloc(h, (void **)&D.status, sizeof(PkStatus) * (size_t)P.n_inst))) return rc;

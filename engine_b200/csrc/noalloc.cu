@@ -43,8 +43,7 @@ struct NaLayout {
     static constexpr size_t Z = col_part + na_al(sizeof(double4) * NA_TILES * NA_BW);
     static constexpr size_t local_part = Z + na_al(sizeof(double4) * NA_MAX_CIRCLES);
     static constexpr size_t fin_items = local_part + na_al(sizeof(double4) * NA_MAX_CIRCLES);
-    static constexpr size_t item_primal = fin_items + na_al(sizeof(int2) * NA_NB);
-    static constexpr size_t blk_primal = item_primal + na_al(sizeof(double) * 2 * NA_ITEMS);
+    static constexpr size_t blk_primal = fin_items + na_al(sizeof(int2) * NA_NB);
     static constexpr size_t blk_dual = blk_primal + na_al(sizeof(double) * 4 * NA_NB);
     static constexpr size_t status = blk_dual + na_al(sizeof(double) * 4 * NA_NB);
     static constexpr size_t wall_vp = status + na_al(sizeof(PkStatus));
@@ -214,7 +213,6 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     D.local_part = (double4 *)(base + NaLayout::local_part);
     D.fin_items = (const int2 *)(base + NaLayout::fin_items);
     D.n_fin = s_inst.nb;
-    D.item_primal = (double *)(base + NaLayout::item_primal);
     D.blk_primal = (double *)(base + NaLayout::blk_primal);
     D.blk_dual = (double *)(base + NaLayout::blk_dual);
     D.status = (PkStatus *)(base + NaLayout::status);
@@ -250,7 +248,6 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     PDM_CUDA(cudaMemcpyAsync((void *)D.rad_coef, s_rad_coef, sizeof(float4) * N, cudaMemcpyHostToDevice, s));
     PDM_CUDA(cudaMemcpyAsync((void *)D.rad_rho, s_rad_rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     PDM_CUDA(cudaMemcpyAsync((void *)D.fin_items, s_fin, sizeof(int2) * s_inst.nb, cudaMemcpyHostToDevice, s));
-    PDM_CUDA(cudaMemsetAsync(D.item_primal, 0, sizeof(double) * 2 * n_items, s));
     PDM_CUDA(cudaMemsetAsync(D.blk_primal, 0, sizeof(double) * 4 * s_inst.nb, s));
     PDM_CUDA(cudaMemsetAsync(D.blk_dual, 0, sizeof(double) * 4 * s_inst.nb, s));
     // consensus: caller's [cx, cy, r] rows -> the kernel's (cx, cy, r, -) rows

@@ -115,16 +115,15 @@ struct PkDev {
     const int *claim;        // [n_items] order in which blocks claim items (largest first)
     int n_inst, n_items, n_circ, pad;
     float *tiles;            // pair state
-    double4 *row_part;       // [tile][BW] sums of M over the row circle's pair edges
+    double4 *row_part;       // [tile][BW] sums of M over the row circle's pair edges; w: their primal-residual sum
     double4 *col_part;       // [tile][BW] same for the column circle
     double4 *Z;              // [circle] consensus (cx, cy, r, -)
     const double4 *Z0;       // [circle] the instance's plain start (fallback target)
     float4 *Zp;              // [circle] Z of the previous sweep (FP32: the values the pass used)
     float *aux;              // N of the pair edges for PK_MODE_N (tile layout; graph handles only)
-    double4 *local_part;     // [circle] rho-weighted wall + radius contributions
+    double4 *local_part;     // [circle] rho-weighted wall + radius contributions; w: their primal-residual sum
     const int2 *fin_items;   // [n_fin] consensus items (instance, circle block)
     int n_fin, pad2;
-    double *item_primal;     // [2][n_items] primal-residual partials by sweep parity
     double *blk_primal;      // [4][n_fin] per consensus item, by sweep index mod 4
     double *blk_dual;        // [4][n_fin]
     PkStatus *status;        // [n_inst]
