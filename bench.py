@@ -21,6 +21,10 @@ Arms:
                     with its -Ofast flags) on all host cores, on a bounded
                     sample of the workload.
 
+Also reported (single GPU): time_to_residual, the batched workload (512
+instances, N in [20, 400]) solved to r + s <= 1e-5 from the plain start and
+from the set-MLP warm start (inference included), host wall clock.
+
 Multi-GPU (torchrun, one process per GPU): every rank solves its own
 instance (replicas, weak scaling; the path has no cross-instance exchange);
 value = all ranks' edge-updates / max-over-ranks device time.
@@ -112,6 +116,7 @@ class Clocks:
 
 
 def dist_init():
+    """One process per GPU over NCCL; gloo on a host without CUDA (tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -120,9 +125,18 @@ def dist_init():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     return world, rank, local
+
+
+def _on_gpu() -> bool:
+    import torch.distributed as dist
+    return dist.get_backend() == "nccl"
 
 
 def barrier(world):
@@ -130,7 +144,8 @@ def barrier(world):
         import torch
         import torch.distributed as dist
         dist.barrier()
-        torch.cuda.synchronize()
+        if _on_gpu():
+            torch.cuda.synchronize()
 
 
 def allreduce_max(world, x: float) -> float:
@@ -138,7 +153,7 @@ def allreduce_max(world, x: float) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if _on_gpu() else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -218,6 +233,43 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------ GPU arm
+TTR_INSTANCES, TTR_SEED, TTR_MAXITER, TTR_TOL, TTR_BUDGET = 512, 900000, 20000, 1e-5, 3000
+
+
+def run_ttr(local: int):
+    """Time to residual on the batched workload: 512 instances (N uniform in
+    [20, 400], box aspect uniform in [1, 2]), host wall clock from the solve
+    call until every instance has r + s <= 1e-5 or used its iteration cap.
+    plain: the batch handle's plain start.  learned: set-MLP features and
+    forward, warm start, then one solve in which instances not converged
+    after TTR_BUDGET sweeps restart from their plain start in the same launch
+    (and get the plain path's full cap).  Both run once untimed first."""
+    import numpy as np
+
+    from engine_b200 import learned
+    inst = learned.make_instances(TTR_INSTANCES, TTR_SEED)
+    net = learned.SetMLP(device=local)
+    net.load()
+    for _ in range(2):
+        pl = learned.solve_plain(inst, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local)
+        le = learned.solve_learned(inst, net, budget=TTR_BUDGET, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local)
+    net.close()
+    tot_p = sum(float(c[:, 2].sum()) for c in pl["circles"])
+    tot_l = sum(float(c[:, 2].sum()) for c in le["circles"])
+    its_p = np.array([x["iterations"] for x in pl["stats"]])
+    its_l = np.array([x["iterations"] for x in le["stats"]])
+    return {"workload": f"{TTR_INSTANCES} packing instances, N uniform in [20,400], aspect uniform in [1,2], "
+                        f"seeded Gaussian-code plain starts (seed {TTR_SEED})",
+            "tol": TTR_TOL, "maxiter": TTR_MAXITER, "learned_budget": TTR_BUDGET,
+            "plain_s": pl["wall_s"], "learned_s": le["wall_s"], "speedup": pl["wall_s"] / le["wall_s"],
+            "converged_plain": int(sum(x["converged"] for x in pl["stats"])),
+            "converged_learned": int(sum(x["converged"] for x in le["stats"])),
+            "fallbacks": le["fallbacks"],
+            "median_sweeps_plain": int(np.median(its_p)), "median_sweeps_learned": int(np.median(its_l)),
+            "total_radius_rel_diff": (tot_l - tot_p) / tot_p,
+            "max_violation_learned": max(float(x["max_violation"]) for x in le["stats"])}
+
+
 def run_e2e(args, local: int):
     """updateGOpenMP(G, sweeps, threads) on a host graph of the workload."""
     import engine_b200 as eb
@@ -286,6 +338,12 @@ def run_engine_arm(args):
             e2e["value"] = world * (-e2e_v)
         except Exception as ex:  # report, never fake
             e2e = {"value": None, "unit": METRIC, "error": str(ex)[:200]}
+    ttr = None
+    if world == 1 and not args.no_ttr and n == N_CIRCLES:
+        try:
+            ttr = run_ttr(local)
+        except Exception as ex:  # report, never fake
+            ttr = {"error": str(ex)[:200]}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and n == N_CIRCLES:
         threads = os.cpu_count() or 1
@@ -317,6 +375,7 @@ def run_engine_arm(args):
                          "kernel": "pk_persistent"},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "time_to_residual": ttr,
             "gpu_launches": launches,
             "clocks": ck,
             "wall_s": wall,
@@ -342,6 +401,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ttr", action="store_true", help="skip the batched time-to-residual comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

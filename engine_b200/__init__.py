@@ -143,6 +143,7 @@ _SIGS = {
     "paradmm_gpu_instance_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "paradmm_gpu_set_fallback": (C.c_int, [C.c_void_p, C.c_int64]),
+    "paradmm_gpu_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_int]),
     "paradmm_gpu_instance_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "paradmm_gpu_pin_graph": (C.c_int, [C.POINTER(Graph)]),
@@ -196,10 +197,15 @@ def last_error() -> str:
 
 
 def opts(**kw) -> Opts:
+    """paradmm_gpu_opts with defaults; coop_min_n sets reserved[0] (per-instance
+    schedule: the smallest instance solved by a whole cluster)."""
     o = Opts()
     load().paradmm_gpu_default_opts(C.byref(o))
     for k, v in kw.items():
-        setattr(o, k, v)
+        if k == "coop_min_n":
+            o.reserved[0] = int(v)
+        else:
+            setattr(o, k, v)
     return o
 
 
@@ -432,7 +438,8 @@ class Handle:
         return out
 
     def phase_times(self) -> list[float]:
-        """Mean block time per sweep (us): pass, barrier 1, finalise, barrier 2."""
+        """Mean block time per sweep (us): pass, barrier 1, finalise, barrier 2
+        (per-instance schedule: pass, barrier, consensus, barrier + stop test)."""
         out = (C.c_double * 4)()
         check(self.lib.paradmm_gpu_phase_times(self.ptr, out))
         return list(out)

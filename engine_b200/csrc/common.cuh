@@ -29,6 +29,7 @@ struct DevCtl {
     unsigned int item_ctr[2]; // dynamic work counters, one per iteration parity
     unsigned int pad[2];      // pad[0]: sweeps completed by the launch
     unsigned long long prof[4];  // optional: summed block time in pass, barrier 1, finalise, barrier 2 (ns)
+    unsigned long long timeout_ns;  // barrier wait limit (0: PDM_BARRIER_TIMEOUT_NS)
     unsigned int grp_count[PDM_BAR_GROUPS][32];  // per-group arrivals, one 128-B line each
 };
 
@@ -71,7 +72,7 @@ PDM_D int ld_volatile_i32(const int *p) { return *(const volatile int *)p; }
 // on one of PDM_BAR_GROUPS group counters (separate cache lines); the last
 // block of each group arrives on the root counter, and the last root arrival
 // releases everyone by bumping the generation.  Every wait is bounded by
-// PDM_BARRIER_TIMEOUT_NS and PDM_BARRIER_MAX_POLLS; on timeout, or when
+// ctl->timeout_ns (default PDM_BARRIER_TIMEOUT_NS) and PDM_BARRIER_MAX_POLLS; on timeout, or when
 // another block has already recorded an error, it returns false and the
 // caller leaves its loop.  All threads of the block get the same answer.
 PDM_D bool grid_barrier(DevCtl *ctl)
@@ -99,11 +100,12 @@ PDM_D bool grid_barrier(DevCtl *ctl)
             }
         }
         if (!releaser) {
+            const uint64_t limit = ctl->timeout_ns ? ctl->timeout_ns : PDM_BARRIER_TIMEOUT_NS;
             const uint64_t t0 = globaltimer_ns();
             uint64_t polls = 0;
             while (ld_acquire_u32(&ctl->bar_gen) == gen) {
                 if (ld_volatile_i32(&ctl->err) != DEV_OK) { ok = 0; break; }
-                if (++polls > PDM_BARRIER_MAX_POLLS || globaltimer_ns() - t0 > PDM_BARRIER_TIMEOUT_NS) {
+                if (++polls > PDM_BARRIER_MAX_POLLS || globaltimer_ns() - t0 > limit) {
                     atomicCAS(&ctl->err, DEV_OK, DEV_BARRIER_TIMEOUT);
                     ok = 0;
                     break;

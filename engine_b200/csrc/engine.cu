@@ -485,6 +485,26 @@ static int pk_finalize_build(paradmm_gpu *h)
     return PARADMM_OK;
 }
 
+// Plain/warm state of every instance from its Z: one launch over all
+// instances (grid.y = instance) when the grid allows it.
+static int pk_init_all(paradmm_gpu *h, int radius_duals)
+{
+    PkHost &P = *h->pk;
+    long long slots = 0;
+    for (int i = 0; i < P.n_inst; ++i) slots = std::max(slots, (long long)P.inst[i].nb * (P.inst[i].nb + 1) / 2 * P.BW * P.BW);
+    const int grid = (int)std::max(1LL, std::min<long long>(h->num_sms * 4, slots / 256 + 1));
+    for (int i = 0; i < P.n_inst; ++i) {
+        if (P.n_inst > 65535 || i == 0) {
+            cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, nullptr, grid, h->stream, radius_duals);
+            if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
+        }
+        P.nmode[i] = PK_MODE_Z;
+        P.upload_iter[i] = P.it_next;
+    }
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    return PARADMM_OK;
+}
+
 static int pk_init_instance_state(paradmm_gpu *h, int inst, const float *d_pair_duals)
 {
     PkHost &P = *h->pk;
@@ -576,7 +596,7 @@ extern "C" int paradmm_gpu_create_packing(const paradmm_packing_desc *descs, int
     P.dynamic = 1;
     for (int i = 0; i < count; ++i) pk_add_desc(P, descs[i], i);
     rc = pk_finalize_build(h);
-    for (int i = 0; rc == PARADMM_OK && i < count; ++i) rc = pk_init_instance_state(h, i, nullptr);
+    if (rc == PARADMM_OK) rc = pk_init_all(h, 0);
     if (rc) { free_handle_memory(h); delete h->pk; delete h; return rc; }
     h->num_dims = 2;
     *out = h;
@@ -783,6 +803,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     R.tol = tol;
     R.check_every = check_every < 1 ? 1 : check_every;
     R.fallback_after = P.fallback_after < n ? P.fallback_after : 0;
+    R.prof = P.prof;
     PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
     cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, &h->ctl->item_ctr[0],
                                         P.inst_grid, P.cluster, h->stream);
@@ -790,10 +811,13 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     ++h->launches;
     PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
     PDM_CUDA(cudaMemcpyAsync(st.data(), P.D.status, sizeof(PkStatus) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(&c, h->ctl, sizeof c, cudaMemcpyDeviceToHost, h->stream));
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     float t = 0;
     cudaEventElapsedTime(&t, h->ev0, h->ev1);
     if (ms) *ms = t;
+    if (P.prof && c.pad[1] > 0)  // mean CTA time per sweep: pass, sync, consensus, sync + stop test
+        for (int q = 0; q < 4; ++q) P.phase_us[q] = (double)c.prof[q] / 1e3 / (double)c.pad[1];
     int rc = PARADMM_OK;
     for (int i = 0; i < P.n_inst; ++i) {
         const long long ran = st[i].last_iter - it0 + 1;
@@ -1353,20 +1377,7 @@ extern "C" int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles,
     std::vector<double4> z(P.n_circ);
     for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(circles[3 * g], circles[3 * g + 1], circles[3 * g + 2], 0.0);
     PDM_CUDA(cudaMemcpyAsync(P.D.Z, z.data(), sizeof(double4) * P.n_circ, cudaMemcpyHostToDevice, h->stream));
-    // one launch over all instances (grid.y = instance) when the grid allows it
-    long long slots = 0;
-    for (int i = 0; i < P.n_inst; ++i) slots = std::max(slots, (long long)P.inst[i].nb * (P.inst[i].nb + 1) / 2 * P.BW * P.BW);
-    const int grid = (int)std::max(1LL, std::min<long long>(h->num_sms * 4, slots / 256 + 1));
-    for (int i = 0; i < P.n_inst; ++i) {
-        if (P.n_inst > 65535 || i == 0) {
-            cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, nullptr, grid, h->stream, radius_duals);
-            if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
-        }
-        P.nmode[i] = PK_MODE_Z;
-        P.upload_iter[i] = P.it_next;
-    }
-    PDM_CUDA(cudaStreamSynchronize(h->stream));
-    return PARADMM_OK;
+    return pk_init_all(h, radius_duals);
 }
 
 extern "C" int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps)
@@ -1559,4 +1570,38 @@ extern "C" void updateGOpenMP(graph *G, int maxiter, int numthreads)
     (void)numthreads;
     if (maxiter <= 0) return;
     sweep_call(G, -1, maxiter);
+}
+
+// ===========================================================================
+// Failure detection self-test: a grid barrier one block never reaches.
+// ===========================================================================
+__global__ void pdm_barrier_probe(DevCtl *ctl)
+{
+    if (blockIdx.x == gridDim.x - 1) return;  // this block never arrives
+    grid_barrier(ctl);
+}
+
+extern "C" int paradmm_gpu_selftest_barrier_timeout(int device, int timeout_ms)
+{
+    ok_status();
+    if (timeout_ms < 1 || timeout_ms > 10000) return pdm_set_error(PARADMM_EINVAL, "timeout_ms must be in [1, 10000]");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return pdm_set_error(PARADMM_ENODEVICE, "no CUDA device %d", device);
+    DevGuard guard(device);
+    DevCtl *d = nullptr;
+    PDM_CUDA(cudaMalloc(&d, sizeof(DevCtl)));
+    DevCtl c{};
+    c.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
+    cudaError_t e = cudaMemcpy(d, &c, sizeof c, cudaMemcpyHostToDevice);
+    void *args[] = {(void *)&d};
+    if (e == cudaSuccess) e = cudaLaunchCooperativeKernel((const void *)pdm_barrier_probe, dim3(2), dim3(32), args, 0, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&c, d, sizeof c, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "barrier self-test", __FILE__, __LINE__);
+    if (c.err == DEV_BARRIER_TIMEOUT)
+        return pdm_set_error(PARADMM_ETIMEOUT, "grid barrier wait ran out after %d ms (self-test: one block never arrives)",
+                             timeout_ms);
+    return pdm_set_error(PARADMM_ECUDA, "barrier self-test: the missing block was not detected (device error %d)", c.err);
 }

@@ -190,6 +190,14 @@ int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps);
  * solve call, else 0. */
 int paradmm_gpu_instance_fallbacks(const paradmm_gpu *h, int *restarted);
 
+/* Failure-detection self-test (no reference counterpart): launches a
+ * two-block grid barrier that one block never reaches, with a wait limit of
+ * timeout_ms.  The waiting block gives up after the limit, records the
+ * device-side error and returns, as the packing kernels do when a block
+ * stops making progress; the call then returns PARADMM_ETIMEOUT, the status
+ * paradmm_gpu_solve reports in that case.  The device stays usable. */
+int paradmm_gpu_selftest_barrier_timeout(int device, int timeout_ms);
+
 /* Device memory the handle holds, in bytes. */
 int64_t paradmm_gpu_device_bytes(const paradmm_gpu *h);
 
@@ -202,8 +210,10 @@ int64_t paradmm_gpu_launches(const paradmm_gpu *h);
 
 /* Packing engine: when on, later sweeps record how long the average block
  * spends per sweep in the pass, the first grid barrier, the consensus
- * finalisation and the second barrier; paradmm_gpu_phase_times returns those
- * four means (microseconds) for the last solve/iterate call. */
+ * finalisation and the second barrier (per-instance schedule: the pass, the
+ * block/cluster barrier after it, the consensus, and the barrier plus stop
+ * test); paradmm_gpu_phase_times returns those four means (microseconds)
+ * for the last solve/iterate call. */
 int paradmm_gpu_set_profiling(paradmm_gpu *h, int on);
 int paradmm_gpu_phase_times(const paradmm_gpu *h, double out[4]);
 

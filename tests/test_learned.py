@@ -143,3 +143,29 @@ def test_fallback_needs_instance_schedule():
         b.set_fallback(10)
     b.set_fallback(0)
     b.close()
+
+
+def test_trained_network_reduces_sweeps():
+    """The committed weights on fresh instances of the batched workload
+    (N uniform in [20, 400]): the learned warm start (with the in-launch
+    fallback) needs fewer sweeps than the plain start, and the packings it
+    converges to are no smaller (total radius) and as feasible."""
+    from engine_b200 import learned
+    inst = learned.make_instances(48, 4242)
+    net = learned.SetMLP()
+    net.load()
+    pl = learned.solve_plain(inst)
+    le = learned.solve_learned(inst, net, budget=3000)
+    net.close()
+    its_p = np.array([x["iterations"] for x in pl["stats"]])
+    its_l = np.array([x["iterations"] for x in le["stats"]])
+    conv_p = np.array([x["converged"] for x in pl["stats"]], bool)
+    conv_l = np.array([x["converged"] for x in le["stats"]], bool)
+    assert conv_l.sum() >= conv_p.sum() - 1
+    assert np.median(its_l) < 0.8 * np.median(its_p), (np.median(its_l), np.median(its_p))
+    tot_p = sum(c[:, 2].sum() for c in pl["circles"])
+    tot_l = sum(c[:, 2].sum() for c in le["circles"])
+    assert (tot_l - tot_p) / tot_p > -1e-3, (tot_l, tot_p)
+    vp = max(x["max_violation"] for x, c in zip(pl["stats"], conv_p) if c)
+    vl = max(x["max_violation"] for x, c in zip(le["stats"], conv_l) if c)
+    assert vl <= max(10 * vp, 1e-4), (vl, vp)
