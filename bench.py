@@ -243,16 +243,24 @@ def run_ttr(local: int):
     plain: the batch handle's plain start.  learned: set-MLP features and
     forward, warm start, then one solve in which instances not converged
     after TTR_BUDGET sweeps restart from their plain start in the same launch
-    (and get the plain path's full cap).  Both run once untimed first."""
+    (and get the plain path's full cap).  Both run once untimed first, on
+    the schedule the autotuner picked for batches of this distribution."""
     import numpy as np
 
     from engine_b200 import learned
     inst = learned.make_instances(TTR_INSTANCES, TTR_SEED)
+    # schedule from the autotuner, tuned on another seeded batch of the same
+    # distribution (probe = full solves to the tolerance; untimed, like
+    # creating the handle), used by both arms
+    b = learned.Batch(learned.make_instances(TTR_INSTANCES, TTR_SEED + 1), device=local)
+    tune = b.autotune(TTR_MAXITER, TTR_TOL)
+    b.close()
+    kw = dict(schedule=tune["schedule"], cluster=tune["cluster_size"], coop_min_n=tune["coop_min_n"])
     net = learned.SetMLP(device=local)
     net.load()
     for _ in range(2):
-        pl = learned.solve_plain(inst, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local)
-        le = learned.solve_learned(inst, net, budget=TTR_BUDGET, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local)
+        pl = learned.solve_plain(inst, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local, **kw)
+        le = learned.solve_learned(inst, net, budget=TTR_BUDGET, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local, **kw)
     net.close()
     tot_p = sum(float(c[:, 2].sum()) for c in pl["circles"])
     tot_l = sum(float(c[:, 2].sum()) for c in le["circles"])
@@ -261,6 +269,9 @@ def run_ttr(local: int):
     return {"workload": f"{TTR_INSTANCES} packing instances, N uniform in [20,400], aspect uniform in [1,2], "
                         f"seeded Gaussian-code plain starts (seed {TTR_SEED})",
             "tol": TTR_TOL, "maxiter": TTR_MAXITER, "learned_budget": TTR_BUDGET,
+            "schedule": {"schedule": "instance" if tune["schedule"] == 2 else "grid", "cluster": tune["cluster_size"],
+                         "coop_min_n": tune["coop_min_n"], "autotune_candidates": tune["candidates"],
+                         "probe_ms_best": tune["ms"], "probe_ms_worst": tune["worst_ms"]},
             "plain_s": pl["wall_s"], "learned_s": le["wall_s"], "speedup": pl["wall_s"] / le["wall_s"],
             "converged_plain": int(sum(x["converged"] for x in pl["stats"])),
             "converged_learned": int(sum(x["converged"] for x in le["stats"])),

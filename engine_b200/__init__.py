@@ -87,6 +87,12 @@ class PackingDesc(C.Structure):
                 ("alpha", C.c_double), ("init", C.POINTER(C.c_double))]
 
 
+class Tuning(C.Structure):
+    """paradmm_gpu_tuning."""
+    _fields_ = [("schedule", C.c_int), ("cluster_size", C.c_int), ("coop_min_n", C.c_int), ("candidates", C.c_int),
+                ("ms", C.c_double), ("worst_ms", C.c_double)]
+
+
 class ParadmmError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"paradmm status {status}: {msg}")
@@ -144,6 +150,7 @@ _SIGS = {
     "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "paradmm_gpu_set_fallback": (C.c_int, [C.c_void_p, C.c_int64]),
     "paradmm_gpu_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_int]),
+    "paradmm_gpu_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     "paradmm_gpu_instance_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "paradmm_gpu_pin_graph": (C.c_int, [C.POINTER(Graph)]),
@@ -204,6 +211,8 @@ def opts(**kw) -> Opts:
     for k, v in kw.items():
         if k == "coop_min_n":
             o.reserved[0] = int(v)
+        elif k == "no_graphs":
+            o.reserved[1] = 1 if v else 0
         else:
             setattr(o, k, v)
     return o
@@ -430,6 +439,13 @@ class Handle:
         """Per-instance schedule: restart unconverged instances from their plain
         start after this many sweeps of a solve call (0: off)."""
         check(self.lib.paradmm_gpu_set_fallback(self.ptr, int(after_sweeps)))
+
+    def autotune(self, sweeps: int = 100, tol: float = -1.0) -> dict:
+        """Times the schedule candidates on a probe solve(sweeps, tol), keeps
+        the fastest (state unchanged).  Returns the chosen configuration."""
+        t = Tuning()
+        check(self.lib.paradmm_gpu_autotune(self.ptr, int(sweeps), float(tol), C.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
     def instance_fallbacks(self) -> np.ndarray:
         """1 for every instance that fell back to its plain start in the last call."""

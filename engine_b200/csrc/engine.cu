@@ -269,6 +269,14 @@ static int dput(paradmm_gpu *h, T **p, const std::vector<T> &v)
 
 static void free_handle_memory(paradmm_gpu *h)
 {
+    if (h->pk) {
+        if (h->pk->graph_exec) cudaGraphExecDestroy(h->pk->graph_exec);
+        if (h->pk->h_status) cudaFreeHost(h->pk->h_status);
+        if (h->pk->h_ctl) cudaFreeHost(h->pk->h_ctl);
+        h->pk->graph_exec = nullptr;
+        h->pk->h_status = nullptr;
+        h->pk->h_ctl = nullptr;
+    }
     for (void *p : h->allocs) cudaFree(p);
     h->allocs.clear();
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -351,6 +359,31 @@ static int pick_V(const paradmm_gpu_opts &o, int maxN)
 
 // Allocates and uploads everything of a packing handle whose host tables
 // (inst, items, circ, walls, rads, init_Z) are filled.
+// Per-instance schedule parameters.  Large instances are the critical path
+// of a batch: the first n_coop of the order (N >= coop_min_n) get a whole
+// cluster of `cluster` CTAs each; the rest run one per CTA.  cluster 0:
+// default (2); a size the device cannot launch falls back to the next
+// smaller one.
+static void pk_set_instance_schedule(paradmm_gpu *h, int cluster, int coop_min_n)
+{
+    PkHost &P = *h->pk;
+    int cl = cluster;
+    if (cl != 1 && cl != 2 && cl != 4 && cl != 8) cl = 2;
+    int nclu = 0;
+    while (cl > 1 && (pk_instances_max_clusters(P.V, P.stream_hint, cl, &nclu) != cudaSuccess || nclu < 1)) {
+        cudaGetLastError();
+        cl /= 2;
+    }
+    P.cluster = cl;
+    int ib = 0;
+    if (pk_instances_blocks_per_sm(P.V, P.stream_hint, &ib) != cudaSuccess || ib < 1) ib = 1;
+    P.inst_grid = cl > 1 ? nclu * cl : h->num_sms * ib;
+    P.coop_min_n = coop_min_n > 0 ? coop_min_n : 200;
+    P.n_coop = 0;
+    if (cl > 1)
+        for (int q = 0; q < P.n_inst && P.inst[P.order[q]].N >= P.coop_min_n; ++q) P.n_coop = q + 1;
+}
+
 static int pk_finalize_build(paradmm_gpu *h)
 {
     PkHost &P = *h->pk;
@@ -455,27 +488,11 @@ static int pk_finalize_build(paradmm_gpu *h)
         if (req == PARADMM_SCHEDULE_INSTANCE && small) P.schedule = PARADMM_SCHEDULE_INSTANCE;
         else if (req == PARADMM_SCHEDULE_GRID || !small) P.schedule = PARADMM_SCHEDULE_GRID;
         else P.schedule = P.n_inst >= 8 ? PARADMM_SCHEDULE_INSTANCE : PARADMM_SCHEDULE_GRID;
-        std::vector<int> order(P.n_inst);
-        for (int i = 0; i < P.n_inst; ++i) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return P.inst[a].N > P.inst[b].N; });
-        if ((rc = dput(h, &P.d_order, order))) return rc;
-        // Large instances are the critical path of a batch: they get a whole
-        // cluster each; the rest run one per CTA.
-        int cl = h->opts.cluster_size;
-        if (cl != 1 && cl != 2 && cl != 4 && cl != 8) cl = 4;
-        int nclu = 0;
-        while (cl > 1 && (pk_instances_max_clusters(P.V, P.stream_hint, cl, &nclu) != cudaSuccess || nclu < 1)) {
-            cudaGetLastError();
-            cl /= 2;
-        }
-        P.cluster = cl;
-        int ib = 0;
-        if (pk_instances_blocks_per_sm(P.V, P.stream_hint, &ib) != cudaSuccess || ib < 1) ib = 1;
-        P.inst_grid = cl > 1 ? nclu * cl : h->num_sms * ib;
-        P.coop_min_n = h->opts.reserved[0] > 0 ? h->opts.reserved[0] : 200;
-        P.n_coop = 0;
-        if (cl > 1)
-            for (int q = 0; q < P.n_inst && P.inst[order[q]].N >= P.coop_min_n; ++q) P.n_coop = q + 1;
+        P.order.resize(P.n_inst);
+        for (int i = 0; i < P.n_inst; ++i) P.order[i] = i;
+        std::stable_sort(P.order.begin(), P.order.end(), [&](int a, int b) { return P.inst[a].N > P.inst[b].N; });
+        if ((rc = dput(h, &P.d_order, P.order))) return rc;
+        pk_set_instance_schedule(h, h->opts.cluster_size, h->opts.reserved[0]);
     }
     P.upload_iter.assign(P.n_inst, 0);
     P.nmode.assign(P.n_inst, PK_MODE_Z);
@@ -596,6 +613,7 @@ extern "C" int paradmm_gpu_create_packing(const paradmm_packing_desc *descs, int
     P.dynamic = 1;
     for (int i = 0; i < count; ++i) pk_add_desc(P, descs[i], i);
     rc = pk_finalize_build(h);
+    P.use_graphs = h->opts.reserved[1] ? 0 : 1;
     if (rc == PARADMM_OK) rc = pk_init_all(h, 0);
     if (rc) { free_handle_memory(h); delete h->pk; delete h; return rc; }
     h->num_dims = 2;
@@ -776,57 +794,116 @@ static int pk_pending_mode(const PkStatus &s, long long last)
 // PK_SWEEPS_PER_LAUNCH sweeps).  Per-instance iteration counts land in
 // P.iters_last_call, statuses in P.status.
 #define PK_SWEEPS_PER_LAUNCH 8192
+// The per-instance launch of one solve call: status in, control block reset,
+// the kernel (with its timing events), status and control block out.  Sweep
+// indices restart at 0 in every call, so the kernel parameters depend only
+// on (n, tol, check_every, fallback, profiling, schedule) and the sequence is
+// captured once into a CUDA graph and replayed by later calls with the same
+// parameters; the status goes through pinned host buffers.
+static int pk_enqueue_instances(paradmm_gpu *h, const PkRun &R, bool capturing)
+{
+    PkHost &P = *h->pk;
+    // in a capture, the timing events must become event-record nodes
+    const unsigned evflags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    PDM_CUDA(cudaMemcpyAsync(P.D.status, P.h_status, sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(DevCtl), h->stream));
+    PDM_CUDA(cudaEventRecordWithFlags(h->ev0, h->stream, evflags));
+    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, &h->ctl->item_ctr[0],
+                                        P.inst_grid, P.cluster, h->stream);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "per-instance packing launch", __FILE__, __LINE__);
+    PDM_CUDA(cudaEventRecordWithFlags(h->ev1, h->stream, evflags));
+    PDM_CUDA(cudaMemcpyAsync(P.h_status, P.D.status, sizeof(PkStatus) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(P.h_ctl, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->stream));
+    return PARADMM_OK;
+}
+
+static void pk_drop_graph(PkHost &P)
+{
+    if (P.graph_exec) cudaGraphExecDestroy(P.graph_exec);
+    P.graph_exec = nullptr;
+}
+
 static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_every, double *ms)
 {
     PkHost &P = *h->pk;
-    const long long it0 = P.it_next;
-    std::vector<PkStatus> st(P.n_inst);
+    if (!P.h_status) {
+        PDM_CUDA(cudaMallocHost((void **)&P.h_status, sizeof(PkStatus) * (size_t)P.n_inst));
+        PDM_CUDA(cudaMallocHost((void **)&P.h_ctl, sizeof(DevCtl)));
+    }
     for (int i = 0; i < P.n_inst; ++i) {
-        PkStatus &s = st[i];
+        PkStatus &s = P.h_status[i];
         s = P.status[i];
         s.last_iter = LLONG_MAX;
-        s.check_from = it0 + 1;
+        s.check_from = 1;
         s.converged = 0;
         s.nonfinite = 0;
         s.nmode = P.nmode[i];
-        s.mode_iter = it0;
+        s.mode_iter = 0;
         s.pad = 0;
         s.t_begin_ns = s.t_end_ns = 0;
     }
-    PDM_CUDA(cudaMemcpyAsync(P.D.status, st.data(), sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
-    DevCtl c{};
-    PDM_CUDA(cudaMemcpyAsync(h->ctl, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
     PkRun R{};
-    R.it0 = it0;
+    R.it0 = 0;
     R.n_iter = (int)std::min<long long>(n, INT_MAX);
     R.dynamic = 0;
     R.tol = tol;
     R.check_every = check_every < 1 ? 1 : check_every;
     R.fallback_after = P.fallback_after < n ? P.fallback_after : 0;
     R.prof = P.prof;
-    PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
-    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, &h->ctl->item_ctr[0],
-                                        P.inst_grid, P.cluster, h->stream);
-    if (e != cudaSuccess) return pdm_cuda_fail(e, "per-instance packing launch", __FILE__, __LINE__);
+    PkGraphKey key;
+    memset(&key, 0, sizeof key);
+    key.n_iter = R.n_iter;
+    key.tol = tol;
+    key.check_every = R.check_every;
+    key.fallback_after = R.fallback_after;
+    key.prof = R.prof;
+    key.cluster = P.cluster;
+    key.n_coop = P.n_coop;
+    key.inst_grid = P.inst_grid;
+    if (P.use_graphs && (!P.graph_exec || memcmp(&key, &P.graph_key, sizeof key) != 0)) {
+        pk_drop_graph(P);
+        cudaGraph_t g = nullptr;
+        int rc = PARADMM_OK;
+        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = pk_enqueue_instances(h, R, true);
+            e = cudaStreamEndCapture(h->stream, &g);
+        }
+        if (e == cudaSuccess && rc == PARADMM_OK) e = cudaGraphInstantiate(&P.graph_exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess || rc != PARADMM_OK) {  // not capturable here: launch directly from now on
+            cudaGetLastError();
+            ok_status();
+            P.graph_exec = nullptr;
+            P.use_graphs = 0;
+        } else {
+            P.graph_key = key;
+        }
+    }
+    if (P.graph_exec) {
+        PDM_CUDA(cudaGraphLaunch(P.graph_exec, h->stream));
+    } else {
+        int rc = pk_enqueue_instances(h, R, false);
+        if (rc) return rc;
+    }
     ++h->launches;
-    PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
-    PDM_CUDA(cudaMemcpyAsync(st.data(), P.D.status, sizeof(PkStatus) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
-    PDM_CUDA(cudaMemcpyAsync(&c, h->ctl, sizeof c, cudaMemcpyDeviceToHost, h->stream));
     PDM_CUDA(cudaStreamSynchronize(h->stream));
+    const DevCtl &c = *P.h_ctl;
     float t = 0;
-    cudaEventElapsedTime(&t, h->ev0, h->ev1);
+    PDM_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
     if (ms) *ms = t;
     if (P.prof && c.pad[1] > 0)  // mean CTA time per sweep: pass, sync, consensus, sync + stop test
         for (int q = 0; q < 4; ++q) P.phase_us[q] = (double)c.prof[q] / 1e3 / (double)c.pad[1];
     int rc = PARADMM_OK;
     for (int i = 0; i < P.n_inst; ++i) {
-        const long long ran = st[i].last_iter - it0 + 1;
+        const PkStatus &st = P.h_status[i];
+        const long long ran = st.last_iter + 1;
         P.iters_last_call[i] = ran > 0 ? ran : 0;
-        P.nmode[i] = pk_pending_mode(st[i], st[i].last_iter);
-        P.status[i] = st[i];
-        if (st[i].nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
+        P.nmode[i] = pk_pending_mode(st, st.last_iter);
+        P.status[i] = st;
+        if (st.nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
     }
-    P.it_next = it0 + n;
+    P.it_next += n;
     return rc;
 }
 
@@ -1378,6 +1455,124 @@ extern "C" int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles,
     for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(circles[3 * g], circles[3 * g + 1], circles[3 * g + 2], 0.0);
     PDM_CUDA(cudaMemcpyAsync(P.D.Z, z.data(), sizeof(double4) * P.n_circ, cudaMemcpyHostToDevice, h->stream));
     return pk_init_all(h, radius_duals);
+}
+
+// ---- schedule autotuner ----
+// Device copies of the state a probe run changes.
+struct PkSnapshot {
+    std::vector<std::pair<void *, size_t>> buf;  // (source, bytes); copies in the same order
+    std::vector<void *> copy;
+    std::vector<int> nmode;
+    std::vector<PkStatus> status;
+    std::vector<long long> iters, upload_iter;
+    long long it_next = 0;
+};
+
+static int pk_snapshot_take(paradmm_gpu *h, PkSnapshot &S)
+{
+    PkHost &P = *h->pk;
+    S.buf = {{P.D.tiles, (size_t)(P.n_tiles * pk_tile_floats(P.BW) * 4LL)},
+             {P.D.Z, sizeof(double4) * (size_t)P.n_circ},
+             {P.D.Zp, sizeof(float4) * (size_t)P.n_circ},
+             {P.D.wall_X, sizeof(float4) * (size_t)std::max(P.n_wall, 1)},
+             {P.D.wall_U, sizeof(float4) * (size_t)std::max(P.n_wall, 1)},
+             {P.D.rad_XU, sizeof(float2) * (size_t)std::max(P.n_rad, 1)}};
+    for (auto &b : S.buf) {
+        void *c = nullptr;
+        cudaError_t e = cudaMalloc(&c, b.second);
+        if (e != cudaSuccess) return pdm_cuda_fail(e, "cudaMalloc (autotune snapshot)", __FILE__, __LINE__);
+        S.copy.push_back(c);
+        PDM_CUDA(cudaMemcpyAsync(c, b.first, b.second, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    S.nmode = P.nmode;
+    S.status = P.status;
+    S.iters = P.iters_last_call;
+    S.upload_iter = P.upload_iter;
+    S.it_next = P.it_next;
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    return PARADMM_OK;
+}
+
+static int pk_snapshot_restore(paradmm_gpu *h, const PkSnapshot &S)
+{
+    PkHost &P = *h->pk;
+    for (size_t q = 0; q < S.buf.size(); ++q)
+        PDM_CUDA(cudaMemcpyAsync(S.buf[q].first, S.copy[q], S.buf[q].second, cudaMemcpyDeviceToDevice, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    P.nmode = S.nmode;
+    P.status = S.status;
+    P.iters_last_call = S.iters;
+    P.upload_iter = S.upload_iter;
+    P.it_next = S.it_next;
+    return PARADMM_OK;
+}
+
+static void pk_snapshot_free(PkSnapshot &S)
+{
+    for (void *c : S.copy) cudaFree(c);
+    S.copy.clear();
+}
+
+extern "C" int paradmm_gpu_autotune(paradmm_gpu *h, int sweeps, double tol, paradmm_gpu_tuning *out)
+{
+    ok_status();
+    if (!h || !h->pk) return pdm_set_error(PARADMM_EINVAL, "autotune needs a packing handle");
+    if (sweeps < 1) return pdm_set_error(PARADMM_EINVAL, "sweeps < 1");
+    DevGuard guard(h->device);
+    PkHost &P = *h->pk;
+    int maxN = 0;
+    for (const PkInst &I : P.inst) maxN = std::max(maxN, I.N);
+    // candidates: (schedule, cluster, coop_min_n)
+    struct Cand { int schedule, cluster, coop; double ms; };
+    std::vector<Cand> cand;
+    cand.push_back({PARADMM_SCHEDULE_GRID, 0, 0, 0});
+    if (maxN <= 1024 && P.n_inst > 1) {
+        cand.push_back({PARADMM_SCHEDULE_INSTANCE, 1, 0, 0});
+        for (int cl : {2, 4})
+            for (int coop : {120, 200, 300})
+                if (maxN >= coop) cand.push_back({PARADMM_SCHEDULE_INSTANCE, cl, coop, 0});
+    }
+    const int saved_schedule = P.schedule, saved_cluster = P.cluster, saved_coop = P.coop_min_n;
+    const int saved_fallback = P.fallback_after;
+    P.fallback_after = 0;
+    PkSnapshot snap;
+    int rc = pk_snapshot_take(h, snap);
+    int best = -1;
+    for (size_t q = 0; rc == PARADMM_OK && q < cand.size(); ++q) {
+        Cand &c = cand[q];
+        P.schedule = c.schedule;
+        if (c.schedule == PARADMM_SCHEDULE_INSTANCE) pk_set_instance_schedule(h, c.cluster, c.coop);
+        if ((rc = pk_snapshot_restore(h, snap))) break;
+        double ms = 0;
+        rc = pk_run(h, sweeps, tol, h->opts.check_every, &ms);
+        if (rc == PARADMM_ENONFINITE) rc = PARADMM_OK;  // timing only
+        c.ms = ms;
+        if (rc == PARADMM_OK && (best < 0 || ms < cand[best].ms)) best = (int)q;
+    }
+    int rc2 = snap.copy.size() == snap.buf.size() ? pk_snapshot_restore(h, snap) : PARADMM_OK;
+    pk_snapshot_free(snap);
+    P.fallback_after = saved_fallback;
+    if (rc == PARADMM_OK) rc = rc2;
+    if (rc != PARADMM_OK || best < 0) {
+        P.schedule = saved_schedule;
+        if (saved_schedule == PARADMM_SCHEDULE_INSTANCE) pk_set_instance_schedule(h, saved_cluster, saved_coop);
+        return rc != PARADMM_OK ? rc : pdm_set_error(PARADMM_ECUDA, "autotune: no configuration ran");
+    }
+    const Cand &b = cand[best];
+    P.schedule = b.schedule;
+    if (b.schedule == PARADMM_SCHEDULE_INSTANCE) pk_set_instance_schedule(h, b.cluster, b.coop);
+    if (out) {
+        memset(out, 0, sizeof *out);
+        out->schedule = P.schedule;
+        out->cluster_size = P.schedule == PARADMM_SCHEDULE_INSTANCE ? P.cluster : 0;
+        out->coop_min_n = P.schedule == PARADMM_SCHEDULE_INSTANCE ? P.coop_min_n : 0;
+        out->ms = b.ms;
+        out->candidates = (int)cand.size();
+        double worst = 0;
+        for (const Cand &c : cand) worst = std::max(worst, c.ms);
+        out->worst_ms = worst;
+    }
+    return PARADMM_OK;
 }
 
 extern "C" int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps)

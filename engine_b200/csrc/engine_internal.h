@@ -26,6 +26,13 @@ struct GraphInfo {
     std::vector<int> circle_of_var;           // -1 if none
 };
 
+// Parameters a captured per-instance launch was built for.
+struct PkGraphKey {
+    int n_iter;
+    double tol;
+    int check_every, fallback_after, prof, cluster, n_coop, inst_grid;
+};
+
 struct PkHost {
     int V = 2, BW = 64;
     bool stream_hint = true;
@@ -56,9 +63,16 @@ struct PkHost {
     int cluster = 1;                 // CTAs per large instance in the per-instance schedule
     int coop_min_n = 0;              // instances with N >= this are solved by a whole cluster
     int n_coop = 0;                  // how many instances that is (the first n_coop of the order)
-    int *d_order = nullptr;          // instances, largest first (per-instance schedule)
+    std::vector<int> order;          // instances, largest first (per-instance schedule)
+    int *d_order = nullptr;          // the same on the device
     int prof = 0;                    // per-phase timing requested
     int fallback_after = 0;          // per-instance schedule: restart from the plain start after this many sweeps
+    // per-instance schedule: the solve call's launch sequence as a CUDA graph
+    int use_graphs = 1;
+    cudaGraphExec_t graph_exec = nullptr;
+    PkGraphKey graph_key{};
+    PkStatus *h_status = nullptr;    // pinned status staging
+    DevCtl *h_ctl = nullptr;         // pinned control-block copy
     double phase_us[4] = {0, 0, 0, 0};  // last call: mean block time per sweep (us)
     // reference-layout maps (graph handles)
     int2 *d_pmap = nullptr; long long n_pmap = 0;

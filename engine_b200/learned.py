@@ -96,13 +96,14 @@ def _descs(instances):
 class Batch:
     """A packing handle over a list of instances (plain start)."""
 
-    def __init__(self, instances, device=0, schedule=0, cluster=0, coop_min_n=0):
+    def __init__(self, instances, device=0, schedule=0, cluster=0, coop_min_n=0, no_graphs=False):
         from . import opts
         self.lib = load()
         self.instances = instances
         arr, self._keep = _descs(instances)
         o = opts(device=device, schedule=schedule, cluster_size=cluster)
         o.reserved[0] = coop_min_n
+        o.reserved[1] = 1 if no_graphs else 0
         p = C.c_void_p()
         check(self.lib.paradmm_gpu_create_packing(arr, len(instances), C.byref(o), C.byref(p)))
         self.h = p
@@ -127,6 +128,12 @@ class Batch:
             check(self.lib.paradmm_gpu_get_circles(self.h, i, c.ctypes.data_as(_P)))
             out.append(c)
         return out
+
+    def autotune(self, sweeps: int = 100, tol: float = -1.0) -> dict:
+        from . import Tuning
+        t = Tuning()
+        check(self.lib.paradmm_gpu_autotune(self.h, int(sweeps), float(tol), C.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
     def set_fallback(self, after_sweeps: int) -> None:
         check(self.lib.paradmm_gpu_set_fallback(self.h, int(after_sweeps)))
@@ -250,8 +257,8 @@ def generate(n: int, seed: int, batch: int = 512, maxiter: int = 20000, tol: flo
     return inst_all, tgt_all
 
 
-def solve_plain(instances, maxiter=20000, tol=1e-5, device=0):
-    b = Batch(instances, device=device)
+def solve_plain(instances, maxiter=20000, tol=1e-5, device=0, **batch_kw):
+    b = Batch(instances, device=device, **batch_kw)
     t = time.perf_counter()
     s = b.solve(maxiter, tol)
     wall = time.perf_counter() - t
@@ -261,11 +268,11 @@ def solve_plain(instances, maxiter=20000, tol=1e-5, device=0):
     return dict(wall_s=wall, device_ms=s["device_ms"], stats=st, circles=circ)
 
 
-def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, radius_duals=1, device=0):
+def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, radius_duals=1, device=0, **batch_kw):
     """Learned path: network proposal -> warm start -> one solve in which every
     instance still unconverged after `budget` sweeps restarts from its plain
     start (in the same launch) and gets the plain path's full maxiter."""
-    b = Batch(instances, device=device)
+    b = Batch(instances, device=device, **batch_kw)
     t = time.perf_counter()
     net.set_data(instances)
     prop = net.predict()

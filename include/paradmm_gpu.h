@@ -73,8 +73,9 @@ typedef struct paradmm_gpu_opts {
     int ctas_per_sm;  /* packing engine: resident CTAs per SM; 0 = tuned       */
     int check_every;  /* sweeps between residual-based stopping checks; 0 = 1  */
     int schedule;     /* packing engine: PARADMM_SCHEDULE_*                      */
-    int cluster_size; /* per-instance schedule: CTAs per large instance (1, 2, 4, 8); 0 = tuned */
-    int reserved[6];  /* reserved[0]: per-instance schedule, smallest N solved by a whole cluster (0 = 200) */
+    int cluster_size; /* per-instance schedule: CTAs per large instance (1, 2, 4, 8); 0 = default (2) */
+    int reserved[6];  /* reserved[0]: per-instance schedule, smallest N solved by a whole cluster (0 = 200);
+                         reserved[1]: 1 = launch per-instance solves directly, not as a replayed CUDA graph */
 } paradmm_gpu_opts;
 
 /* How the packing engine spreads a handle's instances over the GPU. */
@@ -189,6 +190,27 @@ int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps);
 /* restarted[i] = 1 if instance i fell back to its plain start in the last
  * solve call, else 0. */
 int paradmm_gpu_instance_fallbacks(const paradmm_gpu *h, int *restarted);
+
+/* Schedule autotuner (no reference counterpart).  Times each candidate
+ * configuration of the handle -- the grid-wide schedule, and for batches of
+ * instances with N <= 1024 the per-instance schedule with clusters of 1, 2
+ * or 4 CTAs for instances of at least 120, 200 or 300 circles -- on a probe
+ * solve from the handle's current state, restores that state after each
+ * probe, and keeps the fastest.  The probe is paradmm_gpu_solve(h, sweeps,
+ * tol): with tol < 0 every instance runs `sweeps` sweeps (a throughput
+ * probe); with tol >= 0 instances stop on their residual as in a real solve,
+ * which also weighs how long each instance runs.  The state, iteration
+ * counters and fallback setting are as before the call.  Device memory for
+ * one copy of the state is allocated for the duration. */
+typedef struct paradmm_gpu_tuning {
+    int schedule;      /* PARADMM_SCHEDULE_GRID or PARADMM_SCHEDULE_INSTANCE  */
+    int cluster_size;  /* per-instance schedule: CTAs per large instance      */
+    int coop_min_n;    /* per-instance schedule: smallest N given a cluster   */
+    int candidates;    /* configurations timed                                */
+    double ms;         /* device time of the chosen configuration's probe     */
+    double worst_ms;   /* slowest candidate's probe                           */
+} paradmm_gpu_tuning;
+int paradmm_gpu_autotune(paradmm_gpu *h, int sweeps, double tol, paradmm_gpu_tuning *out);
 
 /* Failure-detection self-test (no reference counterpart): launches a
  * two-block grid barrier that one block never reaches, with a wait limit of

@@ -327,3 +327,58 @@ def test_batched_solve_with_retiring_instances_equals_single(schedule):
         assert batched[i]["iterations"] == single["iterations"], (i, batched[i], single)
         assert batched[i]["converged"] == single["converged"], i
         assert np.array_equal(circ[i], c1), i
+
+
+def test_autotune_keeps_state_and_picks_a_valid_schedule():
+    """The schedule autotuner probes each candidate from a snapshot of the
+    state and restores it: a solve after tuning equals the same solve on a
+    fresh handle built with the chosen configuration, bit for bit."""
+    rng = np.random.default_rng(3)
+    descs = []
+    for i in range(24):
+        n = int(rng.integers(12, 260))
+        asp = float(rng.uniform(1, 2))
+        descs.append(dict(n_circles=n, walls=eb.box_walls(asp, 1.0), exponent=2.0, rho=10.0, rho_radius=5.0,
+                          alpha=1.0, init=eb.seeded_circles(n, asp, 1.0, 0.05, 500 + i)))
+    h = eb.Handle.packing(descs)
+    t = h.autotune(30)
+    assert t["candidates"] >= 2 and t["schedule"] in (eb.SCHEDULE_GRID, eb.SCHEDULE_INSTANCE)
+    assert 0 < t["ms"] <= t["worst_ms"]
+    s1 = h.solve(200, 1e-5)
+    c1 = [h.circles(i, d["n_circles"]) for i, d in enumerate(descs)]
+    kw = dict(schedule=t["schedule"])
+    if t["schedule"] == eb.SCHEDULE_INSTANCE:
+        kw.update(cluster_size=t["cluster_size"], coop_min_n=t["coop_min_n"])
+    g = eb.Handle.packing(descs, **kw)
+    s2 = g.solve(200, 1e-5)
+    c2 = [g.circles(i, d["n_circles"]) for i, d in enumerate(descs)]
+    assert s1["iterations"] == s2["iterations"]
+    for a, b in zip(c1, c2):
+        assert np.array_equal(a, b)
+    h.close()
+    g.close()
+
+
+def test_graph_replayed_solves_equal_direct_launches():
+    """Per-instance solves replay a captured CUDA graph once their parameters
+    repeat; repeated solves give the same results as direct launches, and
+    each call launches one kernel."""
+    descs = []
+    for i in range(10):
+        n = 15 + 9 * i
+        descs.append(dict(n_circles=n, walls=eb.box_walls(1.3, 1.0), exponent=2.0, rho=10.0, rho_radius=5.0,
+                          alpha=1.0, init=eb.seeded_circles(n, 1.3, 1.0, 0.05, 40 + i)))
+    out = []
+    for no_graphs in (False, True):
+        h = eb.Handle.packing(descs, schedule=eb.SCHEDULE_INSTANCE, no_graphs=no_graphs)
+        l0 = h.launches()
+        res = []
+        for _ in range(4):
+            h.solve(60, 1e-5)
+            res.append([h.circles(i, d["n_circles"]).copy() for i, d in enumerate(descs)])
+        assert h.launches() - l0 == 4
+        out.append(res)
+        h.close()
+    for ra, rb in zip(*out):
+        for a, b in zip(ra, rb):
+            assert np.array_equal(a, b)
