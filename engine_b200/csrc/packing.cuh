@@ -42,8 +42,10 @@
 // r_i, cx_j, cy_j, r_j, sit in 16-byte chunks: chunk q/4 of lane l at float
 // (q/4) * 128 + 4 l (pk_uoff).  So the warp moves a row as 3V/2 fully
 // coalesced 512-byte segments and each lane touches only its own chunks.
-// Diagonal tiles only use col > row; slots outside the triangle or past N
-// are never touched.
+// A diagonal tile (I, I) with n circles is stored folded (pk_pair_row_slot):
+// storage row t holds circle t's pairs (t, c) at slot c - 1 and circle
+// n - 1 - t's pairs at slot n - 1 - c, so its ceil(n / 2) storage rows are
+// full.  Slots past N are never touched.
 #pragma once
 
 #include <stdint.h>
@@ -160,6 +162,16 @@ PDM_HD int pk_mode_at(int nmode, long long mode_iter, long long k)
     if (k == mode_iter) return nmode;
     if (k == mode_iter + 1 && nmode == PK_MODE_N) return PK_MODE_XN;
     return PK_MODE_RECOMPUTE;
+}
+
+// Storage row and slot of pair (i, j), i < j, local to tile (I, J) with nI
+// circles in block I: (i, j) for an off-diagonal tile, the folded position
+// for a diagonal one.
+PDM_HD void pk_pair_row_slot(bool diag, int nI, int i, int j, int &row, int &slot)
+{
+    if (!diag) { row = i; slot = j; }
+    else if (i < (nI + 1) / 2) { row = i; slot = j - 1; }
+    else { row = nI - 1 - i; slot = nI - 1 - j; }
 }
 
 // Float offset of (component, column) within a tile row (layout above).
