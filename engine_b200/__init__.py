@@ -150,6 +150,7 @@ _SIGS = {
     "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "paradmm_gpu_set_fallback": (C.c_int, [C.c_void_p, C.c_int64]),
     "paradmm_gpu_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_int]),
+    "paradmm_gpu_register_op_source": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
     "paradmm_gpu_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     "paradmm_gpu_instance_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),

@@ -32,6 +32,7 @@ CU_SOURCES = {
     "generic_kernels.cu": ["-fmad=false"],
     "noalloc.cu": [],
     "setmlp.cu": [],
+    "userops.cu": [],
 }
 C_SOURCES = {"graph.c": ["-O2", "-std=gnu11", "-fPIC", "-ffp-contract=off"]}
 

@@ -3,6 +3,7 @@
 //
 // Replaces the reference GPU back-end's host code (core/paradmm-gpu.cu:424-532
 // copyGraphFromCPUtoGPU and the launch loop of packing/gpu.cu:257-291).
+#include <ctype.h>
 #include <dlfcn.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -87,6 +88,43 @@ extern "C" int paradmm_gpu_register_op(paradmm_op_fn op, int kind)
     return PARADMM_OK;
 }
 
+// Operators with a device twin given as source, compiled at run time.
+struct UserOp {
+    void *host;
+    std::string src, name;
+    unsigned long long gen;  // registration generation (a re-registration changes it)
+};
+static std::vector<UserOp> g_user_ops;
+static unsigned long long g_user_gen = 0;
+
+extern "C" int paradmm_gpu_register_op_source(paradmm_op_fn op, const char *device_source, const char *function_name)
+{
+    ok_status();
+    if (!op || !device_source || !function_name || !*function_name)
+        return pdm_set_error(PARADMM_EINVAL, "paradmm_gpu_register_op_source: NULL argument");
+    for (const char *c = function_name; *c; ++c)
+        if (!(isalnum((unsigned char)*c) || *c == '_'))
+            return pdm_set_error(PARADMM_EINVAL, "paradmm_gpu_register_op_source: '%s' is not an identifier", function_name);
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    for (UserOp &u : g_user_ops)
+        if (u.host == (void *)op) {
+            u.src = device_source;
+            u.name = function_name;
+            u.gen = ++g_user_gen;
+            return PARADMM_OK;
+        }
+    g_user_ops.push_back({(void *)op, device_source, function_name, ++g_user_gen});
+    return PARADMM_OK;
+}
+
+static int user_op_index(paradmm_op_fn f)
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    for (size_t i = 0; i < g_user_ops.size(); ++i)
+        if (g_user_ops[i].host == (void *)f) return (int)i;
+    return -1;
+}
+
 static int kind_of_name(const char *s)
 {
     if (!s) return PARADMM_OP_UNKNOWN;
@@ -109,6 +147,8 @@ static int op_kind(paradmm_op_fn f)
         std::lock_guard<std::mutex> lk(g_reg_mu);
         for (auto &p : g_reg)
             if (p.first == (void *)f) return p.second;
+        for (const UserOp &u : g_user_ops)
+            if (u.host == (void *)f) return PARADMM_OP_USER;
     }
     Dl_info info;
     if (f && dladdr((void *)f, &info) && info.dli_saddr == (void *)f) return kind_of_name(info.dli_sname);
@@ -137,7 +177,8 @@ static int analyze_graph(const graph *G, GraphInfo &gi, bool need_state)
         if (k == PARADMM_OP_UNKNOWN)
             return pdm_set_error(PARADMM_EUNSUPPORTED_OP,
                                  "factor %d: operator %p is not one of the packing operators "
-                                 "(register the caller's copy with paradmm_gpu_register_op)",
+                                 "(register the caller's copy with paradmm_gpu_register_op, or give its device "
+                                 "twin with paradmm_gpu_register_op_source)",
                                  f, (void *)G->list_of_operators_functions_pointers[f]);
         const int nv = G->operatorix_to_numedges[f];
         const int *el = G->operatorix_to_edgelistix[f];
@@ -162,6 +203,8 @@ static int analyze_graph(const graph *G, GraphInfo &gi, bool need_state)
     // ---- packing structure ----
     auto no = [&](const char *why) { gi.packing_ok = 0; gi.packing_why = why; return PARADMM_OK; };
     if (d != 2) return no("num_dims is not 2");
+    for (int f = 0; f < G->num_opts; ++f)
+        if (gi.kind[f] == PARADMM_OP_USER) return no("a factor uses a run-time compiled operator");
     const int V = G->num_vars;
     std::vector<int> role(V, 0), partner(V, -1);  // role 1 centre, 2 radius
     auto couple = [&](int c, int r) -> bool {
@@ -1030,6 +1073,50 @@ static int gen_build(paradmm_gpu *h, const graph *G, const GraphInfo &gi, bool f
     if ((rc = dalloc(h, (void **)&Gh.d_viol, sizeof(unsigned long long)))) return rc;
     if (gi.packing_ok)
         for (int c = 0; c < gi.N; ++c) Gh.radius_vars.push_back(gi.radius_var[c]);
+
+    // factors with run-time compiled operators: their ids, compact operator
+    // ids, parameter bytes (16-byte aligned copies), and the compiled X phase
+    std::vector<int> ufac, uid(G->num_opts, -1);
+    std::vector<long long> upoff(G->num_opts, -1);
+    std::vector<unsigned char> ubytes;
+    std::vector<std::pair<std::string, std::string>> ops;
+    std::vector<int> reg_to_compact;
+    for (int f = 0; f < G->num_opts; ++f) {
+        if (kind[f] != PARADMM_OP_USER) continue;
+        const int r = user_op_index(G->list_of_operators_functions_pointers[f]);
+        if (r < 0) return pdm_set_error(PARADMM_EUNSUPPORTED_OP, "factor %d: operator was unregistered", f);
+        if ((int)reg_to_compact.size() <= r) reg_to_compact.resize(r + 1, -1);
+        if (reg_to_compact[r] < 0) {
+            std::lock_guard<std::mutex> lk(g_reg_mu);
+            for (const auto &o : ops)
+                if (o.second == g_user_ops[r].name)
+                    return pdm_set_error(PARADMM_EINVAL, "two operators of the graph use the device name '%s'", o.second.c_str());
+            reg_to_compact[r] = (int)ops.size();
+            ops.emplace_back(g_user_ops[r].src, g_user_ops[r].name);
+        }
+        uid[f] = reg_to_compact[r];
+        ufac.push_back(f);
+        const void *prm = G->list_of_operators_param_pointers ? G->list_of_operators_param_pointers[f] : nullptr;
+        if (prm) {
+            const int bytes = G->list_of_operators_param_sizes ? G->list_of_operators_param_sizes[f] : 0;
+            if (bytes <= 0)
+                return pdm_set_error(PARADMM_EINVAL, "factor %d: a run-time compiled operator's params need their byte size "
+                                     "(addNodeWithParamSize)", f);
+            upoff[f] = (long long)ubytes.size();
+            ubytes.insert(ubytes.end(), (const unsigned char *)prm, (const unsigned char *)prm + bytes);
+            ubytes.resize((ubytes.size() + 15) & ~(size_t)15, 0);
+        }
+    }
+    if (!ufac.empty()) {
+        if (!fp64) return pdm_set_error(PARADMM_EUNSUPPORTED_GRAPH, "run-time compiled operators need the FP64 generic engine");
+        Gh.n_user = (int)ufac.size();
+        if ((rc = dput(h, &Gh.d_user_f, ufac))) return rc;
+        if ((rc = dput(h, &Gh.d_user_id, uid))) return rc;
+        if ((rc = dput(h, &Gh.d_user_poff, upoff))) return rc;
+        if (ubytes.empty()) ubytes.resize(16, 0);
+        if ((rc = dput(h, &Gh.d_user_params, ubytes))) return rc;
+        if ((rc = pdm_user_kernel(ops, h->device, &Gh.user_kernel))) return rc;
+    }
     return PARADMM_OK;
 }
 
@@ -1083,9 +1170,15 @@ static int gen_download(paradmm_gpu *h, graph *G)
 
 static int gen_phase(paradmm_gpu *h, int phase)
 {
-    cudaError_t e = gen_launch_phase(h->gen->D, phase, h->stream);
+    GenHost &Gh = *h->gen;
+    cudaError_t e = gen_launch_phase(Gh.D, phase, h->stream);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "generic phase kernel", __FILE__, __LINE__);
     ++h->launches;
+    if (Gh.n_user > 0 && (phase == GEN_PHASE_X || phase == GEN_PHASE_XM)) {
+        e = pdm_launch_user_x(Gh.user_kernel, Gh.D, Gh, phase == GEN_PHASE_XM, h->stream);
+        if (e != cudaSuccess) return pdm_cuda_fail(e, "run-time compiled operator kernel", __FILE__, __LINE__);
+        ++h->launches;
+    }
     return PARADMM_OK;
 }
 

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -84,6 +85,13 @@ struct PkHost {
 
 struct GenHost {
     GenDev D{};
+    // factors with run-time compiled operators (PARADMM_OP_USER)
+    int n_user = 0;
+    int *d_user_f = nullptr;         // their factor ids
+    int *d_user_id = nullptr;        // [factor] index of the operator in the compiled module
+    long long *d_user_poff = nullptr;  // [factor] byte offset into d_user_params, -1 if none
+    unsigned char *d_user_params = nullptr;
+    const void *user_kernel = nullptr;  // cudaKernel_t of the compiled X-phase
     std::vector<int> radius_vars;    // for the total-radius metric
     double *d_Zprev = nullptr;
     double *d_acc = nullptr;         // residual sums
@@ -91,6 +99,12 @@ struct GenHost {
     int zprev_valid = 0;
     double last_primal = -1, last_dual = -1;
 };
+
+// Run-time compiled operators (userops.cu): the X-phase kernel for operators
+// given as (device source, function name), and its launch over the handle's
+// user factors.
+int pdm_user_kernel(const std::vector<std::pair<std::string, std::string>> &ops, int device, const void **kernel);
+cudaError_t pdm_launch_user_x(const void *kernel, const GenDev &D, const GenHost &Gh, int with_m, cudaStream_t s);
 
 struct paradmm_gpu {
     int engine = PARADMM_ENGINE_AUTO;

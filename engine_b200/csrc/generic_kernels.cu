@@ -116,6 +116,7 @@ __global__ void gen_x(GenDev G, int with_m)
         T *x = X + e0 * d;
         const T *n = Nn + e0 * d;
         const double *rh = G.RHOS + e0;
+        if (kind == PARADMM_OP_USER) continue;  // run-time compiled operators: their own kernel
         if (kind == PARADMM_OP_PAIR) gen_op_pair<T>(x, n, rh, nv, d);
         else if (kind == PARADMM_OP_WALL) gen_op_wall<T>(x, n, rh, nv, d, prm);
         else gen_op_radius<T>(x, n, rh, nv, d, prm);
@@ -212,7 +213,7 @@ __global__ void gen_violation(GenDev G, unsigned long long *out)
             double g = 0;
             for (int k = 0; k < d; ++k) g += prm[k] * (G.Z[d * c + k] - prm[d + k]);
             m = fmax(m, g + G.Z[d * r]);
-        } else {
+        } else if (kind == PARADMM_OP_RADIUS) {
             for (int i = 0; i < G.f_nv[f]; ++i) m = fmax(m, -G.Z[d * (long long)G.e2v[e0 + i]]);
         }
     }

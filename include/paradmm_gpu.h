@@ -52,8 +52,10 @@ enum {
     PARADMM_OP_PAIR = 1,   /* disk_collision_variable_radius, 4 edges          */
     PARADMM_OP_WALL = 2,   /* disk_plane_collision_variable_radius, 2 edges,
                               params = [v (numdims), p (numdims)] doubles     */
-    PARADMM_OP_RADIUS = 3  /* maximize_sum_of_squared_disk_radii_alpha, any
+    PARADMM_OP_RADIUS = 3, /* maximize_sum_of_squared_disk_radii_alpha, any
                               number of edges, params[0] = exponent           */
+    PARADMM_OP_USER = 4    /* a caller's operator with a device twin given as
+                              source (paradmm_gpu_register_op_source)         */
 };
 
 /* ---- engine selection ---- */
@@ -103,6 +105,25 @@ void paradmm_gpu_default_opts(paradmm_gpu_opts *opts);
  * graphs built with the caller's own copy of that operator are accepted.
  * The library's exported operators (paradmm.h) are known without this. */
 int paradmm_gpu_register_op(paradmm_op_fn op, int kind);
+
+/* Any other operator: the caller gives the device twin of host operator
+ * `op` as CUDA C++ source defining
+ *     __device__ void <function_name>(double *x, double *n, double *rhos,
+ *                                     int numvars, int numdims, void *params)
+ * with the reference operator contract (core/paradmm.h:41: read n and rhos,
+ * write x; it may write rhos).  This replaces the reference GPU back-end's
+ * user-supplied __device__ operators called through device function pointers
+ * (core/paradmm-gpu.cu:23-47, packing/gpu.cu:177-184).  The source is
+ * compiled at run time (NVRTC, for this device, FP64 without FMA
+ * contraction, as the generic engine itself is built) the first time a
+ * graph uses it; graphs with such factors run on the generic FP64 engine,
+ * every phase on the GPU.  A factor's params are copied to the device by the
+ * byte size given to addNodeWithParamSize (a factor with params but no size
+ * is rejected with PARADMM_EINVAL), each copy 16-byte aligned.  Errors: the
+ * compiler's log is in paradmm_last_error_string() (PARADMM_EINVAL);
+ * PARADMM_EUNSUPPORTED_OP when the run-time compiler cannot be loaded.
+ * Registering the same `op` again replaces its source. */
+int paradmm_gpu_register_op_source(paradmm_op_fn op, const char *device_source, const char *function_name);
 
 /* Builds a handle for graph G: classifies its factors, lays out the state on
  * the device and uploads the state arrays (X, N, U, Z, RHOS, ALPHAS) that G
