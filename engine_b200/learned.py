@@ -287,3 +287,38 @@ def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, 
     circ = b.circles()
     b.close()
     return dict(wall_s=wall, device_ms=s["device_ms"], stats=st, circles=circ, fallbacks=int(fb.sum()), proposal=prop)
+
+
+def train_weights(n_instances: int = 16384, epochs: int = 40, seed: int = 100000, out: str = WEIGHTS,
+                  device: int = 0) -> dict:
+    """Reproduces the committed weights: converged packings of n_instances
+    seeded instances of the batched workload (plain solver, tol 1e-5), 90 %
+    for training and 10 % for validation, `epochs` Adam passes in batches of
+    32 instances, learning rate 1e-3 decaying to 5e-5, network seed 7."""
+    t = time.perf_counter()
+    inst, tgt = generate(n_instances, seed=seed, device=device)
+    t_gen = time.perf_counter() - t
+    ntr = int(0.9 * len(inst))
+    net = SetMLP(device=device, seed=7)
+    net.set_data(inst[:ntr], tgt[:ntr])
+    t = time.perf_counter()
+    losses = net.train(epochs=epochs, batch_inst=32, lr=1e-3, lr_end=5e-5)
+    t_train = time.perf_counter() - t
+    train_loss = net.eval()
+    net.set_data(inst[ntr:], tgt[ntr:])
+    val_loss = net.eval()
+    net.save(out)
+    net.close()
+    return dict(converged=len(inst), requested=n_instances, generate_s=t_gen, train_s=t_train,
+                train_loss=train_loss, val_loss=val_loss, first_epoch_loss=float(losses[0]), out=out)
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the set-MLP warm start on packings the plain solver produces")
+    ap.add_argument("--instances", type=int, default=16384)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--out", default=WEIGHTS)
+    a = ap.parse_args()
+    print(json.dumps(train_weights(a.instances, a.epochs, out=a.out)))
