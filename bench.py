@@ -233,7 +233,11 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------ GPU arm
-TTR_INSTANCES, TTR_SEED, TTR_MAXITER, TTR_TOL, TTR_BUDGET = 512, 900000, 20000, 1e-5, 3000
+# learned arm: no fallback budget -- on this workload the warm start converges
+# on more instances than the plain start, and restarting slow ones from the
+# plain start only lengthened the batch (0.43 s with a 3000-sweep budget, 0.36 s
+# without, device time)
+TTR_INSTANCES, TTR_SEED, TTR_MAXITER, TTR_TOL, TTR_BUDGET = 512, 900000, 20000, 1e-5, 0
 
 
 def run_ttr(local: int):
@@ -241,9 +245,9 @@ def run_ttr(local: int):
     [20, 400], box aspect uniform in [1, 2]), host wall clock from the solve
     call until every instance has r + s <= 1e-5 or used its iteration cap.
     plain: the batch handle's plain start.  learned: set-MLP features and
-    forward, warm start, then one solve in which instances not converged
-    after TTR_BUDGET sweeps restart from their plain start in the same launch
-    (and get the plain path's full cap).  Both run once untimed first, on
+    forward, warm start, then one solve (TTR_BUDGET > 0 would restart
+    instances not converged after that many sweeps from their plain start in
+    the same launch).  Both run once untimed first, on
     the schedule the autotuner picked for batches of this distribution."""
     import numpy as np
 

@@ -269,16 +269,18 @@ def solve_plain(instances, maxiter=20000, tol=1e-5, device=0, **batch_kw):
 
 
 def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, radius_duals=1, device=0, **batch_kw):
-    """Learned path: network proposal -> warm start -> one solve in which every
-    instance still unconverged after `budget` sweeps restarts from its plain
-    start (in the same launch) and gets the plain path's full maxiter."""
+    """Learned path: network proposal -> warm start -> one solve.  With
+    budget > 0, every instance still unconverged after `budget` sweeps
+    restarts from its plain start (in the same launch) and gets the plain
+    path's full maxiter; with budget <= 0 there is no fallback and every
+    instance gets maxiter sweeps from the warm start."""
     b = Batch(instances, device=device, **batch_kw)
     t = time.perf_counter()
     net.set_data(instances)
     prop = net.predict()
     b.warm_start(prop, radius_duals)
-    b.set_fallback(budget)
-    s = b.solve(budget + maxiter, tol)
+    b.set_fallback(max(budget, 0))
+    s = b.solve((budget if budget > 0 else 0) + maxiter, tol)
     wall = time.perf_counter() - t
     st = b.stats()
     fb = b.fallbacks()
