@@ -406,7 +406,7 @@ def run_engine_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--block-width", type=int, default=0)

@@ -291,35 +291,53 @@ def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, 
     return dict(wall_s=wall, device_ms=s["device_ms"], stats=st, circles=circ, fallbacks=int(fb.sum()), proposal=prop)
 
 
-def train_weights(n_instances: int = 16384, epochs: int = 40, seed: int = 100000, out: str = WEIGHTS,
-                  device: int = 0) -> dict:
+def train_weights(n_instances: int = 20000, epochs: int = 40, seed: int = 100000, out: str = WEIGHTS,
+                  device: int = 0, net_seeds=(7, 8, 9), val_seed: int = 900001) -> dict:
     """Reproduces the committed weights: converged packings of n_instances
     seeded instances of the batched workload (plain solver, tol 1e-5), 90 %
-    for training and 10 % for validation, `epochs` Adam passes in batches of
-    32 instances, learning rate 1e-3 decaying to 5e-5, network seed 7."""
+    for training and 10 % for the validation loss; one network per seed in
+    net_seeds, `epochs` Adam passes in batches of 32 instances, learning rate
+    1e-3 decaying to 5e-5.  The kept network is the one whose warm start
+    solves a separate validation batch (512 instances, seed val_seed, never
+    the evaluation batch) fastest, host wall clock, no fallback."""
     t = time.perf_counter()
     inst, tgt = generate(n_instances, seed=seed, device=device)
     t_gen = time.perf_counter() - t
     ntr = int(0.9 * len(inst))
-    net = SetMLP(device=device, seed=7)
-    net.set_data(inst[:ntr], tgt[:ntr])
-    t = time.perf_counter()
-    losses = net.train(epochs=epochs, batch_inst=32, lr=1e-3, lr_end=5e-5)
-    t_train = time.perf_counter() - t
-    train_loss = net.eval()
-    net.set_data(inst[ntr:], tgt[ntr:])
-    val_loss = net.eval()
+    val = make_instances(512, val_seed)
+    kw = dict(cluster=2, coop_min_n=200)
+    for _ in range(2):
+        plain = solve_plain(val, device=device, **kw)
+    best = None
+    report = []
+    for ns in net_seeds:
+        net = SetMLP(device=device, seed=ns)
+        net.set_data(inst[:ntr], tgt[:ntr])
+        t = time.perf_counter()
+        net.train(epochs=epochs, batch_inst=32, lr=1e-3, lr_end=5e-5)
+        t_train = time.perf_counter() - t
+        train_loss = net.eval()
+        net.set_data(inst[ntr:], tgt[ntr:])
+        val_loss = net.eval()
+        wall = min(solve_learned(val, net, budget=0, device=device, **kw)["wall_s"] for _ in range(2))
+        report.append(dict(net_seed=ns, train_loss=train_loss, val_loss=val_loss, train_s=t_train,
+                           val_batch_s=wall, val_batch_plain_s=plain["wall_s"]))
+        if best is None or wall < best[0]:
+            best = (wall, ns, net.params())
+        net.close()
+    net = SetMLP(device=device, seed=best[1])
+    net.set_params(best[2])
     net.save(out)
     net.close()
-    return dict(converged=len(inst), requested=n_instances, generate_s=t_gen, train_s=t_train,
-                train_loss=train_loss, val_loss=val_loss, first_epoch_loss=float(losses[0]), out=out)
+    return dict(converged=len(inst), requested=n_instances, generate_s=t_gen, kept_net_seed=best[1],
+                candidates=report, out=out)
 
 
 if __name__ == "__main__":
     import argparse
     import json
     ap = argparse.ArgumentParser(description="train the set-MLP warm start on packings the plain solver produces")
-    ap.add_argument("--instances", type=int, default=16384)
+    ap.add_argument("--instances", type=int, default=20000)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--out", default=WEIGHTS)
     a = ap.parse_args()
