@@ -382,3 +382,28 @@ def test_graph_replayed_solves_equal_direct_launches():
     for ra, rb in zip(*out):
         for a, b in zip(ra, rb):
             assert np.array_equal(a, b)
+
+
+def test_config0_fixed_point():
+    """Configuration 0 (N = 100, unit square) solved to r + s <= 1e-5: the
+    FP64 generic engine stops at the same sweep with the same residuals and
+    metrics as the reference's CPU updateG; the FP32 packing engine reaches
+    the tolerance too, feasible, with total radius near the FP64 one."""
+    N = 100
+    pg, orc, circles = problem(N, 3)
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_GENERIC_F64) as g:
+        s64 = g.solve(20000, 1e-5)
+        st64 = g.stats()
+    n, tr = orc.run(20000, tol=1e-5)
+    m = tr[-1]
+    assert s64["converged"] == 1 and s64["iterations"] == n
+    assert abs(st64["primal"] - m[0]) <= 1e-12 and abs(st64["dual"] - m[1]) <= 1e-12
+    assert abs(st64["max_violation"] - m[2]) <= 1e-12 and abs(st64["total_radius"] - m[3]) <= 1e-9
+    desc = dict(n_circles=N, walls=eb.box_walls(1, 1), exponent=EXP, rho=RHO, rho_radius=RHO_R, alpha=ALPHA,
+                init=circles)
+    with eb.Handle.packing([desc]) as h:
+        s32 = h.solve(20000, 1e-5)
+        st32 = h.instance_stats()[0]
+    assert s32["converged"] == 1 and st32["primal"] + st32["dual"] <= 1e-5
+    assert st32["max_violation"] < 2e-3
+    assert abs(st32["total_radius"] - m[3]) / m[3] < 0.02
