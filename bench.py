@@ -256,10 +256,9 @@ def run_ttr(local: int):
     # schedule from the autotuner, tuned on another seeded batch of the same
     # distribution (probe = full solves to the tolerance; untimed, like
     # creating the handle), used by both arms
-    b = learned.Batch(learned.make_instances(TTR_INSTANCES, TTR_SEED + 1), device=local)
-    tune = b.autotune(TTR_MAXITER, TTR_TOL)
-    b.close()
-    kw = dict(schedule=tune["schedule"], cluster=tune["cluster_size"], coop_min_n=tune["coop_min_n"])
+    tune = learned.tune(learned.make_instances(TTR_INSTANCES, TTR_SEED + 1), TTR_MAXITER, TTR_TOL, device=local)
+    kw = dict(schedule=tune["schedule"], cluster=tune["cluster_size"], coop_min_n=tune["coop_min_n"],
+              block_width=tune["block_width"])
     net = learned.SetMLP(device=local)
     net.load()
     for _ in range(2):
@@ -273,7 +272,8 @@ def run_ttr(local: int):
     return {"workload": f"{TTR_INSTANCES} packing instances, N uniform in [20,400], aspect uniform in [1,2], "
                         f"seeded Gaussian-code plain starts (seed {TTR_SEED})",
             "tol": TTR_TOL, "maxiter": TTR_MAXITER, "learned_budget": TTR_BUDGET,
-            "schedule": {"schedule": "instance" if tune["schedule"] == 2 else "grid", "cluster": tune["cluster_size"],
+            "schedule": {"schedule": "instance" if tune["schedule"] == 2 else "grid", "block_width": tune["block_width"],
+                         "cluster": tune["cluster_size"],
                          "coop_min_n": tune["coop_min_n"], "autotune_candidates": tune["candidates"],
                          "probe_ms_best": tune["ms"], "probe_ms_worst": tune["worst_ms"]},
             "plain_s": pl["wall_s"], "learned_s": le["wall_s"], "speedup": pl["wall_s"] / le["wall_s"],

@@ -90,7 +90,7 @@ class PackingDesc(C.Structure):
 class Tuning(C.Structure):
     """paradmm_gpu_tuning."""
     _fields_ = [("schedule", C.c_int), ("cluster_size", C.c_int), ("coop_min_n", C.c_int), ("candidates", C.c_int),
-                ("ms", C.c_double), ("worst_ms", C.c_double)]
+                ("ms", C.c_double), ("worst_ms", C.c_double), ("block_width", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class ParadmmError(RuntimeError):
@@ -152,6 +152,8 @@ _SIGS = {
     "paradmm_gpu_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_int]),
     "paradmm_gpu_register_op_source": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
     "paradmm_gpu_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
+    "paradmm_gpu_create_packing_tuned": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Opts), C.c_int, C.c_double,
+                                                   C.POINTER(C.c_void_p), C.c_void_p]),
     "paradmm_gpu_instance_fallbacks": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "paradmm_gpu_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "paradmm_gpu_pin_graph": (C.c_int, [C.POINTER(Graph)]),
@@ -351,6 +353,36 @@ class Handle:
         check(lib.paradmm_gpu_create(C.byref(G), C.byref(o), C.byref(p)))
         return cls(p.value, lib)
 
+    @staticmethod
+    def _descs(descs: list[dict]):
+        arr = (PackingDesc * len(descs))()
+        keep = []
+        for i, d in enumerate(descs):
+            walls = np.ascontiguousarray(d["walls"], dtype=np.float64)
+            init = np.ascontiguousarray(d["init"], dtype=np.float64)
+            keep += [walls, init]
+            arr[i].n_circles = int(d["n_circles"])
+            arr[i].n_walls = int(walls.shape[0])
+            arr[i].walls = walls.ctypes.data_as(C.POINTER(C.c_double))
+            arr[i].exponent = float(d.get("exponent", 2.0))
+            arr[i].rho = float(d["rho"])
+            arr[i].rho_radius = float(d["rho_radius"])
+            arr[i].alpha = float(d["alpha"])
+            arr[i].init = init.ctypes.data_as(C.POINTER(C.c_double))
+        return arr, keep
+
+    @classmethod
+    def packing_tuned(cls, descs: list[dict], sweeps: int, tol: float = -1.0, **kw) -> tuple["Handle", dict]:
+        """paradmm_gpu_create_packing_tuned: tile side and schedule from probes."""
+        lib = load()
+        arr, keep = cls._descs(descs)
+        p = C.c_void_p()
+        o = opts(**kw)
+        t = Tuning()
+        check(lib.paradmm_gpu_create_packing_tuned(arr, len(descs), C.byref(o), int(sweeps), float(tol), C.byref(p),
+                                                   C.byref(t)))
+        return cls(p.value, lib), {k: getattr(t, k) for k, _ in Tuning._fields_ if k != "reserved"}
+
     @classmethod
     def packing(cls, descs: list[dict], **kw) -> "Handle":
         """descs: dicts with n_circles, walls (k x 4), exponent, rho, rho_radius, alpha, init (N x 3)."""
@@ -446,7 +478,7 @@ class Handle:
         the fastest (state unchanged).  Returns the chosen configuration."""
         t = Tuning()
         check(self.lib.paradmm_gpu_autotune(self.ptr, int(sweeps), float(tol), C.byref(t)))
-        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+        return {k: getattr(t, k) for k, _ in Tuning._fields_ if k != "reserved"}
 
     def instance_fallbacks(self) -> np.ndarray:
         """1 for every instance that fell back to its plain start in the last call."""

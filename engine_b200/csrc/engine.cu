@@ -1668,6 +1668,48 @@ extern "C" int paradmm_gpu_autotune(paradmm_gpu *h, int sweeps, double tol, para
     return PARADMM_OK;
 }
 
+extern "C" int paradmm_gpu_create_packing_tuned(const paradmm_packing_desc *descs, int count,
+                                                const paradmm_gpu_opts *opts, int sweeps, double tol,
+                                                paradmm_gpu **out, paradmm_gpu_tuning *tuning)
+{
+    ok_status();
+    if (!out) return pdm_set_error(PARADMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    paradmm_gpu_opts o;
+    if (opts) o = *opts;
+    else paradmm_gpu_default_opts(&o);
+    const int widths[2] = {64, 128};
+    paradmm_gpu *best = nullptr;
+    paradmm_gpu_tuning bt{};
+    int rc = PARADMM_OK;
+    for (int w : widths) {
+        if (opts && opts->block_width && opts->block_width != w) continue;  // a fixed width is kept
+        o.block_width = w;
+        paradmm_gpu *h = nullptr;
+        rc = paradmm_gpu_create_packing(descs, count, &o, &h);
+        if (rc) break;
+        paradmm_gpu_tuning t{};
+        rc = paradmm_gpu_autotune(h, sweeps, tol, &t);
+        if (rc) { paradmm_gpu_destroy(h); break; }
+        if (!best || t.ms < bt.ms) {
+            if (best) paradmm_gpu_destroy(best);
+            best = h;
+            bt = t;
+            bt.block_width = w;
+        } else {
+            paradmm_gpu_destroy(h);
+        }
+    }
+    if (rc) {
+        if (best) paradmm_gpu_destroy(best);
+        return rc;
+    }
+    if (!best) return pdm_set_error(PARADMM_EINVAL, "no block width to try (block_width must be 0, 64 or 128)");
+    if (tuning) *tuning = bt;
+    *out = best;
+    return PARADMM_OK;
+}
+
 extern "C" int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps)
 {
     ok_status();

@@ -96,12 +96,12 @@ def _descs(instances):
 class Batch:
     """A packing handle over a list of instances (plain start)."""
 
-    def __init__(self, instances, device=0, schedule=0, cluster=0, coop_min_n=0, no_graphs=False):
+    def __init__(self, instances, device=0, schedule=0, cluster=0, coop_min_n=0, no_graphs=False, block_width=0):
         from . import opts
         self.lib = load()
         self.instances = instances
         arr, self._keep = _descs(instances)
-        o = opts(device=device, schedule=schedule, cluster_size=cluster)
+        o = opts(device=device, schedule=schedule, cluster_size=cluster, block_width=block_width)
         o.reserved[0] = coop_min_n
         o.reserved[1] = 1 if no_graphs else 0
         p = C.c_void_p()
@@ -133,7 +133,7 @@ class Batch:
         from . import Tuning
         t = Tuning()
         check(self.lib.paradmm_gpu_autotune(self.h, int(sweeps), float(tol), C.byref(t)))
-        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+        return {k: getattr(t, k) for k, _ in Tuning._fields_ if k != "reserved"}
 
     def set_fallback(self, after_sweeps: int) -> None:
         check(self.lib.paradmm_gpu_set_fallback(self.h, int(after_sweeps)))
@@ -342,3 +342,18 @@ if __name__ == "__main__":
     ap.add_argument("--out", default=WEIGHTS)
     a = ap.parse_args()
     print(json.dumps(train_weights(a.instances, a.epochs, out=a.out)))
+
+
+def tune(instances, sweeps: int, tol: float, device: int = 0) -> dict:
+    """Tile side and schedule for batches like `instances`
+    (paradmm_gpu_create_packing_tuned with probe solve(sweeps, tol))."""
+    from . import Tuning, opts
+    lib = load()
+    arr, keep = _descs(instances)
+    o = opts(device=device)
+    p = C.c_void_p()
+    t = Tuning()
+    check(lib.paradmm_gpu_create_packing_tuned(arr, len(instances), C.byref(o), int(sweeps), float(tol), C.byref(p),
+                                               C.byref(t)))
+    lib.paradmm_gpu_destroy(p)
+    return {k: getattr(t, k) for k, _ in Tuning._fields_ if k != "reserved"}

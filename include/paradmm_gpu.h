@@ -230,8 +230,18 @@ typedef struct paradmm_gpu_tuning {
     int candidates;    /* configurations timed                                */
     double ms;         /* device time of the chosen configuration's probe     */
     double worst_ms;   /* slowest candidate's probe                           */
+    int block_width;   /* paradmm_gpu_create_packing_tuned: chosen tile side  */
+    int reserved[3];
 } paradmm_gpu_tuning;
 int paradmm_gpu_autotune(paradmm_gpu *h, int sweeps, double tol, paradmm_gpu_tuning *out);
+
+/* paradmm_gpu_create_packing plus the tile shape: builds the instances with
+ * tile sides (block widths) 64 and 128 (or only opts->block_width when it is
+ * set), autotunes each handle's schedule with the same probe as
+ * paradmm_gpu_autotune(h, sweeps, tol), and returns the fastest handle in
+ * its initial state (the others are destroyed).  No reference counterpart. */
+int paradmm_gpu_create_packing_tuned(const paradmm_packing_desc *descs, int count, const paradmm_gpu_opts *opts,
+                                     int sweeps, double tol, paradmm_gpu **out, paradmm_gpu_tuning *tuning);
 
 /* Failure-detection self-test (no reference counterpart): launches a
  * two-block grid barrier that one block never reaches, with a wait limit of

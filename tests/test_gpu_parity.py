@@ -407,3 +407,28 @@ def test_config0_fixed_point():
     assert s32["converged"] == 1 and st32["primal"] + st32["dual"] <= 1e-5
     assert st32["max_violation"] < 2e-3
     assert abs(st32["total_radius"] - m[3]) / m[3] < 0.02
+
+
+def test_create_packing_tuned_picks_tile_side_and_schedule():
+    """paradmm_gpu_create_packing_tuned probes tile sides 64 and 128 and the
+    schedules, keeps the fastest handle in its initial state: its solve
+    equals a fresh handle built with the chosen configuration."""
+    rng = np.random.default_rng(4)
+    descs = []
+    for i in range(16):
+        n = int(rng.integers(20, 200))
+        descs.append(dict(n_circles=n, walls=eb.box_walls(1.2, 1.0), exponent=2.0, rho=10.0, rho_radius=5.0,
+                          alpha=1.0, init=eb.seeded_circles(n, 1.2, 1.0, 0.05, 900 + i)))
+    h, t = eb.Handle.packing_tuned(descs, 20)
+    assert t["block_width"] in (64, 128) and t["candidates"] >= 2
+    h.solve(150, -1.0)
+    c1 = [h.circles(i, d["n_circles"]) for i, d in enumerate(descs)]
+    kw = dict(schedule=t["schedule"], block_width=t["block_width"])
+    if t["schedule"] == eb.SCHEDULE_INSTANCE:
+        kw.update(cluster_size=t["cluster_size"], coop_min_n=t["coop_min_n"])
+    g = eb.Handle.packing(descs, **kw)
+    g.solve(150, -1.0)
+    for i, d in enumerate(descs):
+        assert np.array_equal(c1[i], g.circles(i, d["n_circles"]))
+    h.close()
+    g.close()
