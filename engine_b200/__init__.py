@@ -161,6 +161,15 @@ _SIGS = {
     "paradmm_noalloc_state_bytes": (C.c_int64, [C.c_int, C.c_int]),
     "paradmm_gpu_packing_iterate_noalloc": (C.c_int, [C.POINTER(PackingDesc), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                                       C.c_double, C.POINTER(Stats), C.c_int, C.c_void_p]),
+    "paradmm_gpu_shard_rows": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "paradmm_gpu_create_packing_shard": (C.c_int, [C.POINTER(PackingDesc), C.c_int, C.c_int, C.POINTER(Opts),
+                                                   C.POINTER(C.c_void_p)]),
+    "paradmm_gpu_shard_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+    "paradmm_gpu_shard_start": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int]),
+    "paradmm_gpu_shard_begin": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "paradmm_gpu_shard_end": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "paradmm_gpu_shard_poll": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "paradmm_gpu_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Stats)]),
     "paradmm_last_status": (C.c_int, []),
     "paradmm_last_error_string": (C.c_char_p, []),
     "paradmm_set_sweep_options": (None, [C.POINTER(Opts)]),

@@ -391,6 +391,21 @@ static int add_items(PkHost &P, int inst_id, int N, int nb)
     return n;
 }
 
+// Work items of a shard: the pair tiles of block rows [row_lo, row_hi),
+// then the circle blocks of those rows' circles.
+static int add_items_rows(PkHost &P, int inst_id, int N, int nb, int row_lo, int row_hi, int BW)
+{
+    int n = 0;
+    for (int I = row_lo; I < row_hi; ++I)
+        for (int J = I; J < nb; ++J) { P.items.push_back(make_int4(inst_id, 0, I, J)); ++n; }
+    const int c_end = std::min(N, row_hi * BW);
+    for (int c0 = row_lo * BW; c0 < c_end; c0 += PK_THREADS) {
+        P.items.push_back(make_int4(inst_id, 1, c0, std::min(PK_THREADS, c_end - c0)));
+        ++n;
+    }
+    return n;
+}
+
 // Tile side: 64 circles (two columns per lane) or 128 (four).
 static int pick_V(const paradmm_gpu_opts &o, int maxN)
 {
@@ -555,7 +570,8 @@ static int pk_init_all(paradmm_gpu *h, int radius_duals)
     const int grid = (int)std::max(1LL, std::min<long long>(h->num_sms * 4, slots / 256 + 1));
     for (int i = 0; i < P.n_inst; ++i) {
         if (P.n_inst > 65535 || i == 0) {
-            cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, nullptr, grid, h->stream, radius_duals);
+            cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, nullptr, grid, h->stream, radius_duals,
+                                           P.row_lo, P.row_hi);
             if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
         }
         P.nmode[i] = PK_MODE_Z;
@@ -568,7 +584,7 @@ static int pk_init_all(paradmm_gpu *h, int radius_duals)
 static int pk_init_instance_state(paradmm_gpu *h, int inst, const float *d_pair_duals)
 {
     PkHost &P = *h->pk;
-    cudaError_t e = pk_launch_init(P.V, P.D, inst, d_pair_duals, h->num_sms * 4, h->stream);
+    cudaError_t e = pk_launch_init(P.V, P.D, inst, d_pair_duals, h->num_sms * 4, h->stream, 0, P.row_lo, P.row_hi);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     P.nmode[inst] = PK_MODE_Z;
@@ -584,8 +600,14 @@ static int pk_add_desc(PkHost &P, const paradmm_packing_desc &d, int inst_id)
     I.N = N;
     I.nb = (N + P.BW - 1) / P.BW;
     I.circle_base = (int)P.circ.size();
-    I.tile_base = P.n_tiles;
-    P.n_tiles += (long long)I.nb * (I.nb + 1) / 2;
+    if (P.shard_n > 0) {  // one instance; only the rows [row_lo, row_hi) are stored
+        const long long t_lo = pk_tri(P.row_lo, P.row_lo, I.nb);
+        I.tile_base = -t_lo;
+        P.n_tiles = pk_tri(P.row_hi, P.row_hi, I.nb) - t_lo;
+    } else {
+        I.tile_base = P.n_tiles;
+        P.n_tiles += (long long)I.nb * (I.nb + 1) / 2;
+    }
     const double rho[4] = {d.rho, d.rho, d.rho, d.rho}, al[4] = {d.alpha, d.alpha, d.alpha, d.alpha};
     pair_coefficients(I, rho, al);
     const long long E = (long long)N + 2LL * d.n_walls * N + 4LL * N * (N - 1) / 2;
@@ -619,7 +641,8 @@ static int pk_add_desc(PkHost &P, const paradmm_packing_desc &d, int inst_id)
         P.init_Z.push_back(d.init[3 * c + 1]);
         P.init_Z.push_back(d.init[3 * c + 2]);
     }
-    add_items(P, inst_id, N, I.nb);
+    if (P.shard_n > 0) add_items_rows(P, inst_id, N, I.nb, P.row_lo, P.row_hi, P.BW);
+    else add_items(P, inst_id, N, I.nb);
     P.inst.push_back(I);
     return PARADMM_OK;
 }
@@ -1324,6 +1347,8 @@ extern "C" int paradmm_gpu_solve(paradmm_gpu *h, int maxiter, double tol, paradm
     if (stats) memset(stats, 0, sizeof *stats);
     if (maxiter == 0) return PARADMM_OK;
     if (h->engine != PARADMM_ENGINE_PACKING) return gen_run(h, maxiter, tol, h->opts.check_every, stats);
+    if (h->pk->shard_n > 0)
+        return pdm_set_error(PARADMM_EINVAL, "a shard of an instance sweeps through paradmm_gpu_shard_begin/end only");
     double ms = 0;
     const int rc = pk_run(h, maxiter, tol, h->opts.check_every, &ms);
     if (stats) {
@@ -1610,6 +1635,7 @@ extern "C" int paradmm_gpu_autotune(paradmm_gpu *h, int sweeps, double tol, para
 {
     ok_status();
     if (!h || !h->pk) return pdm_set_error(PARADMM_EINVAL, "autotune needs a packing handle");
+    if (h->pk->shard_n > 0) return pdm_set_error(PARADMM_EINVAL, "a shard of an instance has no schedule to tune");
     if (sweeps < 1) return pdm_set_error(PARADMM_EINVAL, "sweeps < 1");
     DevGuard guard(h->device);
     PkHost &P = *h->pk;
@@ -1729,6 +1755,259 @@ extern "C" int paradmm_gpu_instance_fallbacks(const paradmm_gpu *h, int *restart
     if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
     for (int i = 0; i < h->pk->n_inst; ++i) restarted[i] = h->pk->status[i].pad != 0;
     return PARADMM_OK;
+}
+
+// ===========================================================================
+// One instance sharded over ranks
+// ===========================================================================
+// Pair count of circle-block row I (its tiles (I, J >= I)) plus its circles'
+// wall and radius factors.
+static long long shard_row_cost(int N, int BW, int I)
+{
+    const long long nI = std::min(BW, N - I * BW);
+    const long long right = std::max(0LL, (long long)N - (long long)(I + 1) * BW);
+    return nI * (nI - 1) / 2 + nI * right + nI;
+}
+
+extern "C" int paradmm_gpu_shard_rows(int n_circles, int block_width, int nranks, int *bounds)
+{
+    ok_status();
+    if (!bounds) return pdm_set_error(PARADMM_EINVAL, "bounds is NULL");
+    const int BW = block_width == 128 ? 128 : 64;
+    if (block_width != 0 && block_width != 32 && block_width != 64 && block_width != 128)
+        return pdm_set_error(PARADMM_EINVAL, "block_width %d (0, 64 or 128)", block_width);
+    if (n_circles < 2 || n_circles > 32767) return pdm_set_error(PARADMM_EINVAL, "n_circles %d", n_circles);
+    const int nb = (n_circles + BW - 1) / BW;
+    if (nranks < 1 || nranks > nb)
+        return pdm_set_error(PARADMM_EINVAL, "%d ranks for %d circle-block rows (at most one rank per row)", nranks, nb);
+    std::vector<long long> cum(nb + 1, 0);
+    for (int I = 0; I < nb; ++I) cum[I + 1] = cum[I] + shard_row_cost(n_circles, BW, I);
+    bounds[0] = 0;
+    for (int r = 1; r < nranks; ++r) {
+        // the boundary whose prefix cost is nearest to r / nranks of the total,
+        // leaving at least one row to every rank
+        const double target = (double)cum[nb] * r / nranks;
+        int best = bounds[r - 1] + 1;
+        for (int I = best + 1; I <= nb - (nranks - r); ++I)
+            if (std::fabs((double)cum[I] - target) < std::fabs((double)cum[best] - target)) best = I;
+        bounds[r] = best;
+    }
+    bounds[nranks] = nb;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_create_packing_shard(const paradmm_packing_desc *desc, int rank, int nranks,
+                                                const paradmm_gpu_opts *opts, paradmm_gpu **out)
+{
+    ok_status();
+    if (!out) return pdm_set_error(PARADMM_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (!desc) return pdm_set_error(PARADMM_EINVAL, "desc is NULL");
+    const paradmm_packing_desc &d = *desc;
+    if (d.n_circles < 2 || d.n_circles > 32767 || d.n_walls < 0 || d.n_walls > 8 || (d.n_walls && !d.walls) || !d.init)
+        return pdm_set_error(PARADMM_EINVAL, "bad description (n_circles %d, n_walls %d)", d.n_circles, d.n_walls);
+    if (!(d.rho > 0) || !(d.rho_radius > 0)) return pdm_set_error(PARADMM_EINVAL, "penalties must be positive");
+    if (nranks < 1 || rank < 0 || rank >= nranks) return pdm_set_error(PARADMM_EINVAL, "rank %d of %d", rank, nranks);
+    paradmm_gpu *h = new paradmm_gpu();
+    int rc = handle_init(h, opts);
+    if (rc) { free_handle_memory(h); delete h; return rc; }
+    DevGuard g(h->device);
+    if (h->opts.engine != PARADMM_ENGINE_AUTO && h->opts.engine != PARADMM_ENGINE_PACKING) {
+        free_handle_memory(h); delete h;
+        return pdm_set_error(PARADMM_EUNSUPPORTED_GRAPH, "structured packing problems run on the packing engine only");
+    }
+    h->engine = PARADMM_ENGINE_PACKING;
+    h->pk = new PkHost();
+    PkHost &P = *h->pk;
+    P.V = pick_V(h->opts, d.n_circles);
+    P.BW = 32 * P.V;
+    P.stream_hint = true;
+    P.dynamic = 1;
+    std::vector<int> bounds(nranks + 1);
+    rc = paradmm_gpu_shard_rows(d.n_circles, P.BW, nranks, bounds.data());
+    if (rc == PARADMM_OK) {
+        P.shard_n = nranks;
+        P.shard_rank = rank;
+        P.row_lo = bounds[rank];
+        P.row_hi = bounds[rank + 1];
+        pk_add_desc(P, d, 0);
+        rc = pk_finalize_build(h);
+    }
+    if (rc == PARADMM_OK) {
+        // the shard's pass is a plain launch (no grid barrier): as many CTAs as fit
+        int bps = 0;
+        if (pk_shard_prepare(P.V, P.stream_hint, &bps) != cudaSuccess || bps < 1)
+            rc = pdm_set_error(PARADMM_ECUDA, "shard pass kernel cannot run on this device");
+        else {
+            if (h->opts.ctas_per_sm > 0) bps = std::min(bps, h->opts.ctas_per_sm);
+            P.grid = std::max(1, std::min(h->num_sms * bps, P.n_items));
+        }
+    }
+    if (rc == PARADMM_OK) rc = dalloc(h, (void **)&P.d_done, sizeof(unsigned));
+    if (rc == PARADMM_OK && cudaMemset(P.d_done, 0, sizeof(unsigned)) != cudaSuccess)
+        rc = pdm_set_error(PARADMM_ECUDA, "cudaMemset failed");
+    P.use_graphs = 0;
+    if (rc == PARADMM_OK) rc = pk_init_all(h, 0);
+    if (rc) { free_handle_memory(h); delete h->pk; delete h; return rc; }
+    h->num_dims = 2;
+    *out = h;
+    return PARADMM_OK;
+}
+
+static int shard_handle(paradmm_gpu *h, PkHost **P)
+{
+    if (!h) return pdm_set_error(PARADMM_EINVAL, "handle is NULL");
+    if (!h->pk || h->pk->shard_n < 1) return pdm_set_error(PARADMM_EINVAL, "not a shard (paradmm_gpu_create_packing_shard)");
+    *P = h->pk;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_shard_info(const paradmm_gpu *h, int *row_lo, int *row_hi, int64_t *exchange_bytes)
+{
+    ok_status();
+    if (!h || !h->pk || h->pk->shard_n < 1) return pdm_set_error(PARADMM_EINVAL, "not a shard");
+    if (row_lo) *row_lo = h->pk->row_lo;
+    if (row_hi) *row_hi = h->pk->row_hi;
+    if (exchange_bytes) *exchange_bytes = (int64_t)sizeof(double4) * h->pk->inst[0].N;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_shard_start(paradmm_gpu *h, int maxiter, double tol, int check_every)
+{
+    ok_status();
+    PkHost *Pp;
+    int rc = shard_handle(h, &Pp);
+    if (rc) return rc;
+    PkHost &P = *Pp;
+    if (maxiter < 1) return pdm_set_error(PARADMM_EINVAL, "maxiter < 1");
+    if (P.shard_running) return pdm_set_error(PARADMM_EINVAL, "a run is armed: paradmm_gpu_shard_finish first");
+    DevGuard guard(h->device);
+    const long long it0 = P.it_next;
+    PkStatus s = P.status[0];
+    s.last_iter = LLONG_MAX;
+    s.check_from = it0 + 2;
+    s.converged = 0;
+    s.nonfinite = 0;
+    s.nmode = P.nmode[0];
+    s.mode_iter = it0;
+    PDM_CUDA(cudaMemcpyAsync(P.D.status, &s, sizeof s, cudaMemcpyHostToDevice, h->stream));
+    DevCtl c{};
+    c.n_active = 1;
+    PDM_CUDA(cudaMemcpyAsync(h->ctl, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemsetAsync(P.d_done, 0, sizeof(unsigned), h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    P.shard_it0 = it0;
+    P.shard_k = it0;
+    P.shard_stop = it0 + maxiter;
+    P.shard_tol = tol;
+    P.shard_check_every = check_every < 1 ? 1 : check_every;
+    P.shard_phase = 0;
+    P.shard_running = 1;
+    P.iters_last_call[0] = 0;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_shard_begin(paradmm_gpu *h, void *exchange, void *stream)
+{
+    ok_status();
+    PkHost *Pp;
+    int rc = shard_handle(h, &Pp);
+    if (rc) return rc;
+    PkHost &P = *Pp;
+    if (!P.shard_running || P.shard_phase != 0 || P.shard_k >= P.shard_stop)
+        return pdm_set_error(PARADMM_EINVAL, "no sweep to begin (paradmm_gpu_shard_start / shard_end first)");
+    if (!exchange || ((uintptr_t)exchange & 15u)) return pdm_set_error(PARADMM_EINVAL, "exchange must be a 16-byte aligned device buffer");
+    DevGuard guard(h->device);
+    PkRun R{};
+    R.it0 = P.shard_k;
+    R.n_iter = 1;
+    R.dynamic = 1;
+    R.tol = P.shard_tol;
+    R.check_every = P.shard_check_every;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = pk_launch_shard_begin(P.V, P.stream_hint, P.D, R, P.grid, P.inst[0].nb, P.row_lo, P.row_hi,
+                                          (double4 *)exchange, s);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "shard pass launch", __FILE__, __LINE__);
+    h->launches += 2;
+    P.shard_phase = 1;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_shard_end(paradmm_gpu *h, const void *exchange, void *stream)
+{
+    ok_status();
+    PkHost *Pp;
+    int rc = shard_handle(h, &Pp);
+    if (rc) return rc;
+    PkHost &P = *Pp;
+    if (!P.shard_running || P.shard_phase != 1) return pdm_set_error(PARADMM_EINVAL, "no sweep begun");
+    if (!exchange || ((uintptr_t)exchange & 15u)) return pdm_set_error(PARADMM_EINVAL, "exchange must be a 16-byte aligned device buffer");
+    DevGuard guard(h->device);
+    PkRun R{};
+    R.it0 = P.shard_it0;
+    R.n_iter = (int)std::min<long long>(P.shard_stop - P.shard_it0, INT_MAX);
+    R.dynamic = 1;
+    R.tol = P.shard_tol;
+    R.check_every = P.shard_check_every;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = pk_launch_shard_end(P.V, P.D, R, P.shard_k, P.inst[0].nb, (const double4 *)exchange, P.d_done, s);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "shard consensus launch", __FILE__, __LINE__);
+    ++h->launches;
+    ++P.shard_k;
+    P.shard_phase = 0;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_shard_poll(paradmm_gpu *h, void *stream, int *active)
+{
+    ok_status();
+    PkHost *Pp;
+    int rc = shard_handle(h, &Pp);
+    if (rc) return rc;
+    if (!active) return pdm_set_error(PARADMM_EINVAL, "active is NULL");
+    DevGuard guard(h->device);
+    PDM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    DevCtl c{};
+    PDM_CUDA(cudaMemcpyAsync(&c, h->ctl, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    if (c.err != DEV_OK) return pdm_set_error(PARADMM_ECUDA, "shard kernels: device error %d", c.err);
+    *active = c.n_active > 0 && Pp->shard_k < Pp->shard_stop ? 1 : 0;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_shard_finish(paradmm_gpu *h, void *stream, paradmm_stats *stats)
+{
+    ok_status();
+    PkHost *Pp;
+    int rc = shard_handle(h, &Pp);
+    if (rc) return rc;
+    PkHost &P = *Pp;
+    if (!P.shard_running) return pdm_set_error(PARADMM_EINVAL, "no run armed");
+    if (P.shard_phase != 0) return pdm_set_error(PARADMM_EINVAL, "a sweep waits for its paradmm_gpu_shard_end");
+    DevGuard guard(h->device);
+    PDM_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    PkStatus st{};
+    PDM_CUDA(cudaMemcpyAsync(&st, P.D.status, sizeof st, cudaMemcpyDeviceToHost, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    const long long last = std::min(st.last_iter, P.shard_k - 1);
+    P.iters_last_call[0] = std::max(0LL, last - P.shard_it0 + 1);
+    P.nmode[0] = pk_pending_mode(st, last);
+    P.status[0] = st;
+    P.it_next = P.shard_k;
+    P.shard_running = 0;
+    rc = st.nonfinite ? pdm_set_error(PARADMM_ENONFINITE, "residual became NaN/Inf") : PARADMM_OK;
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->iterations = P.iters_last_call[0];
+        stats->converged = st.converged;
+        stats->status = rc;
+        stats->primal = st.primal;
+        stats->dual = st.dual;
+        stats->device_ms = NAN;
+        stats->max_violation = NAN;
+        stats->total_radius = NAN;
+    }
+    return rc;
 }
 
 extern "C" void paradmm_gpu_destroy(paradmm_gpu *h)

@@ -81,6 +81,14 @@ struct PkHost {
     int2 *d_cmap = nullptr;
     int *d_flag = nullptr;
     unsigned long long *d_viol = nullptr;
+    // shard of one instance (paradmm_gpu_create_packing_shard): this rank
+    // stores the pair tiles of circle-block rows [row_lo, row_hi)
+    int shard_n = 0, shard_rank = 0, row_lo = 0, row_hi = -1;
+    int shard_running = 0, shard_phase = 0;  // a run is armed; 1 = the exchange of sweep shard_k is pending
+    long long shard_it0 = 0, shard_k = 0, shard_stop = 0;  // first sweep of the run, next sweep, end of the run
+    double shard_tol = -1.0;
+    int shard_check_every = 1;
+    unsigned *d_done = nullptr;      // CTAs of the running consensus launch that finished
 };
 
 struct GenHost {

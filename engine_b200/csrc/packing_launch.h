@@ -12,7 +12,7 @@ cudaError_t pk_launch_instances(int V, bool stream_hint, const PkDev &D, const P
 cudaError_t pk_instances_max_clusters(int V, bool stream_hint, int cluster, int *clusters);
 cudaError_t pk_instances_blocks_per_sm(int V, bool stream_hint, int *blocks);
 cudaError_t pk_launch_init(int V, const PkDev &D, int inst, const float *pair_duals, int grid, cudaStream_t s,
-                           int radius_duals = 0);
+                           int radius_duals = 0, int row_lo = 0, int row_hi = -1);
 cudaError_t pk_launch_scatter(int V, const PkDev &D, int inst, const int2 *pmap, long long npairs, const int *wmap,
                               int wall0, int nwall, const int *rmap, int rad0, int nrad, const int2 *cmap,
                               const double *Nd, const double *Ud, const double *Zd, int *flag, int grid, cudaStream_t s);
@@ -21,3 +21,8 @@ cudaError_t pk_launch_gather(int V, const PkDev &D, int inst, const int2 *pmap, 
                              const int *wcirc, const int *rcirc, int nmode, double *Xo, double *Mo, double *No,
                              double *Uo, double *Zo, int grid, cudaStream_t s);
 cudaError_t pk_launch_violation(const PkDev &D, unsigned long long *out, int grid, cudaStream_t s);
+cudaError_t pk_shard_prepare(int V, bool stream_hint, int *blocks_per_sm);
+cudaError_t pk_launch_shard_begin(int V, bool stream_hint, const PkDev &D, const PkRun &R, int grid, int nb,
+                                  int row_lo, int row_hi, double4 *exch, cudaStream_t s);
+cudaError_t pk_launch_shard_end(int V, const PkDev &D, const PkRun &R, long long k, int nb, const double4 *exch,
+                                unsigned *done, cudaStream_t s);

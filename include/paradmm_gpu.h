@@ -287,6 +287,41 @@ int paradmm_gpu_unpin_graph(const graph *G);
  * (packing/host.c:299-335). */
 int paradmm_add_packing_factors(graph *G, int n_circles, int n_walls, double *walls, double *exponent, int order);
 
+/* ---- one packing instance sharded over ranks ----
+ *
+ * No reference counterpart: the reference runs one graph on one device
+ * (core/paradmm-gpu.cu).  An instance is split by circle-block rows: rank r
+ * of nranks stores and sweeps the pair tiles (I, J >= I) of rows
+ * [bounds[r], bounds[r+1]) and the wall and radius factors of those rows'
+ * circles, with bounds from paradmm_gpu_shard_rows (rows balanced by pair
+ * count; block width opts->block_width, 64 by default).  Every rank keeps
+ * the whole consensus Z.  One sweep is
+ *     paradmm_gpu_shard_begin(h, exchange, stream)   pass + this rank's partial sums
+ *     <sum `exchange` over all ranks, in place>      e.g. an NCCL all-reduce (float64 sum)
+ *     paradmm_gpu_shard_end(h, exchange, stream)     consensus + residuals + stop test
+ * where `exchange` is a device buffer of exchange_bytes (32 bytes per
+ * circle, 16-byte aligned) owned by the caller.  Every rank derives Z from
+ * the same summed buffer, so all ranks hold identical Z and take the same
+ * stop decision; with one rank the sweep equals the unsharded engine's bit
+ * for bit.  `stream` is a cudaStream_t (NULL: the default stream); all
+ * three steps must be ordered on it.  A run is armed by shard_start
+ * (maxiter sweeps at most, stop when primal + dual <= tol, tol < 0: never);
+ * shard_poll synchronises the stream and says whether the instance still
+ * runs (all ranks see the same answer after the same sweep); shard_finish
+ * ends the run and fills stats (iterations, converged, residuals).  The
+ * handle answers paradmm_gpu_get_circles / instance_stats / warm_start like
+ * a one-instance packing handle; paradmm_gpu_solve/iterate and the
+ * autotuner refuse it. */
+int paradmm_gpu_shard_rows(int n_circles, int block_width, int nranks, int *bounds /* nranks + 1 */);
+int paradmm_gpu_create_packing_shard(const paradmm_packing_desc *desc, int rank, int nranks,
+                                     const paradmm_gpu_opts *opts, paradmm_gpu **out);
+int paradmm_gpu_shard_info(const paradmm_gpu *h, int *row_lo, int *row_hi, int64_t *exchange_bytes);
+int paradmm_gpu_shard_start(paradmm_gpu *h, int maxiter, double tol, int check_every);
+int paradmm_gpu_shard_begin(paradmm_gpu *h, void *exchange, void *stream);
+int paradmm_gpu_shard_end(paradmm_gpu *h, const void *exchange, void *stream);
+int paradmm_gpu_shard_poll(paradmm_gpu *h, void *stream, int *active);
+int paradmm_gpu_shard_finish(paradmm_gpu *h, void *stream, paradmm_stats *stats);
+
 /* ---- allocation-free packing sweeps ----
  *
  * Some callers cannot allocate device memory while they run: services that
