@@ -27,7 +27,9 @@ from the set-MLP warm start (inference included), host wall clock.
 
 Multi-GPU (torchrun, one process per GPU): every rank solves its own
 instance (replicas, weak scaling; the path has no cross-instance exchange);
-value = all ranks' edge-updates / max-over-ranks device time.
+value = all ranks' edge-updates / max-over-ranks device time.  With
+--mode shard the ranks split ONE instance by circle-block rows and sum a
+32 B/circle buffer per sweep with an NCCL all-reduce (strong scaling).
 """
 from __future__ import annotations
 
@@ -403,6 +405,67 @@ def run_engine_arm(args):
         dist.destroy_process_group()
 
 
+def run_shard_arm(args):
+    """--mode shard: ONE instance split over the ranks by circle-block rows
+    (engine_b200.shard), one all-reduce of 32 B per circle per sweep (NCCL);
+    strong scaling.  Device time: CUDA events on the stream that carries the
+    kernels and the all-reduce, max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    import engine_b200 as eb
+    from engine_b200.shard import Shard, run_sharded
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    n = args.circles
+    desc = dict(n_circles=n, walls=eb.box_walls(BOX_W, BOX_H), exponent=EXPONENT, rho=RHO, rho_radius=RHO_R,
+                alpha=ALPHA, init=seeded_init(n, SEED))
+    sh = Shard(desc, rank, world, device=local, block_width=args.block_width)
+    ex = torch.zeros(sh.exchange_bytes // 8, dtype=torch.float64, device=f"cuda:{local}")
+
+    def allreduce(t):
+        if world > 1:
+            dist.all_reduce(t)
+
+    run_sharded(sh, ex, allreduce, max(3, args.warmup), -1.0, poll_every=64)
+    barrier(world)
+    clocks = Clocks(str(local) if world == 1 else ",".join(str(i) for i in range(world))) if rank == 0 else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = sh.launches()
+    e0.record()
+    st = run_sharded(sh, ex, allreduce, args.steps, -1.0, poll_every=max(64, args.steps))
+    e1.record()
+    torch.cuda.synchronize()
+    launches = sh.launches() - l0
+    barrier(world)
+    ck = clocks.stop() if clocks else None
+    dev_ms = allreduce_max(world, e0.elapsed_time(e1))
+    E = edges_of(n)
+    algo = algo_bytes_per_sweep(n)
+    peak, peak_kind = measured_peak()
+    achieved = algo * args.steps / (dev_ms * 1e-3) / 1e9 / world  # per GPU
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": E * args.steps / (dev_ms * 1e-3), "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": f"ONE plain circle packing N={n}, {BOX_W:g}x{BOX_H:g} box, radii in [0,{RMAX}], "
+                                   f"seeded uniform init, split over the ranks by circle-block rows",
+                       "circles": n, "edges": E, "parallelism": f"shard x{world} (all-reduce of {32 * n} B/sweep)",
+                       "rows": list(sh.rows), "timing": "CUDA events on torch's stream (kernels + all-reduce)"},
+            "iterations_per_s": args.steps / (dev_ms * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": None, "per": "GPU (algorithmic bytes / world)",
+                         "kernel": "pk_shard_pass + pk_shard_partial + pk_shard_consensus"},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": launches, "clocks": ck,
+            "iterations_run": st["iterations"],
+        }
+        print(json.dumps(out), flush=True)
+    sh.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,11 +480,15 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ttr", action="store_true", help="skip the batched time-to-residual comparison")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "shard"],
+                    help="multi-GPU: one instance per rank (default) or one instance split over the ranks")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.mode == "shard":
+        run_shard_arm(args)
     else:
         run_engine_arm(args)
 

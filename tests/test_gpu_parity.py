@@ -131,6 +131,42 @@ def test_packing_teacher_forced_one_sweep(bw):
     print(f"teacher-forced worst max|diff| = {worst:.3e}")
 
 
+@pytest.mark.parametrize("container,exponent", [("triangle", 2.0), ("box", 1.0), ("triangle", 1.5)])
+def test_packing_teacher_forced_containers_and_exponents(container, exponent):
+    """The demo's triangle container (walls with slanted normals,
+    packing/host.c:141-149) and radius exponents 1 (closed-form powers) and
+    1.5 (powf Newton steps), teacher-forced like the box case."""
+    N, seed = 130, 33
+    W, H = (1.0, 0.87) if container == "triangle" else (1.0, 1.0)
+    walls = eb.triangle_walls() if container == "triangle" else eb.box_walls(W, H)
+    circles = eb.seeded_circles(N, W, H, 0.05, seed)
+    pg = eb.PackingGraph(N, walls, exponent)
+    pg.init_seeded(circles, RHO, RHO_R, ALPHA)
+    orc = oracle_lib.OraclePacking(oracle_lib.best(), N, walls, exponent)
+    orc.init(seed, W, H, 0.05, RHO, RHO_R, ALPHA)
+    done, checked = 0, 0
+    for k in (0, 3, 30, 150):
+        orc.run(k - done, trace=False)
+        done = k
+        st = orc.state()
+        if not all(np.isfinite(v).all() for v in st.values()):
+            break
+        for key, v in st.items():
+            pg.G.arr(key)[:] = v
+        with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
+            h.iterate(1)
+            h.download(pg.G)
+        orc.sweep()
+        done += 1
+        ref = orc.state()
+        if not all(np.isfinite(v).all() for v in ref.values()):
+            break
+        d = maxdiff(pg.G.state(), ref)
+        assert d <= TOL_F32, f"k={k}: max diff {d}"
+        checked += 1
+    assert checked >= 2
+
+
 def test_packing_free_running_from_init():
     """Free-running from the random init.  The early phase is chaotic: an
     FP32 re-evaluation of the same formulas on the CPU leaves 1e-4 of the
