@@ -17,6 +17,11 @@ enum : int {
     DEV_BARRIER_TIMEOUT = 1,
 };
 
+static inline const char *pdm_dev_err_name(int e)
+{
+    return e == DEV_BARRIER_TIMEOUT ? "grid barrier" : "unknown";
+}
+
 // Control block of one persistent launch: grid barrier, error flag, work
 // counters.  Lives in device memory owned by the handle; zeroed before each
 // launch.

@@ -955,6 +955,8 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     ++h->launches;
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     const DevCtl &c = *P.h_ctl;
+    if (c.err != DEV_OK)
+        return pdm_set_error(PARADMM_ETIMEOUT, "packing kernel: a device-side wait ran out (%s)", pdm_dev_err_name(c.err));
     float t = 0;
     PDM_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
     if (ms) *ms = t;
@@ -1022,7 +1024,7 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
         cudaEventElapsedTime(&t, h->ev0, h->ev1);
         total_ms += t;
         if (c.err != DEV_OK)
-            return pdm_set_error(PARADMM_ETIMEOUT, "packing kernel: a grid barrier wait ran out (device error %d)", c.err);
+            return pdm_set_error(PARADMM_ETIMEOUT, "packing kernel: a device-side wait ran out (%s)", pdm_dev_err_name(c.err));
         const long long sweeps = (long long)c.pad[0];
         if (P.prof && sweeps > 0)
             for (int q = 0; q < 4; ++q) P.phase_us[q] = (double)c.prof[q] / 1e3 / P.grid / (double)sweeps;
@@ -1970,7 +1972,8 @@ extern "C" int paradmm_gpu_shard_poll(paradmm_gpu *h, void *stream, int *active)
     DevCtl c{};
     PDM_CUDA(cudaMemcpyAsync(&c, h->ctl, sizeof c, cudaMemcpyDeviceToHost, h->stream));
     PDM_CUDA(cudaStreamSynchronize(h->stream));
-    if (c.err != DEV_OK) return pdm_set_error(PARADMM_ECUDA, "shard kernels: device error %d", c.err);
+    if (c.err != DEV_OK)
+        return pdm_set_error(PARADMM_ETIMEOUT, "shard kernels: a device-side wait ran out (%s)", pdm_dev_err_name(c.err));
     *active = c.n_active > 0 && Pp->shard_k < Pp->shard_stop ? 1 : 0;
     return PARADMM_OK;
 }

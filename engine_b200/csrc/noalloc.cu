@@ -86,11 +86,15 @@ static int64_t na_tiles_of(int n)
     return (int64_t)nb * (nb + 1) / 2;
 }
 
+// Radius (X, U) pairs of n circles, padded so the FP32 circles after them
+// start on a 16-byte boundary.
+static int64_t na_rad_bytes(int n) { return ((int64_t)n * (int64_t)sizeof(float2) + 15) & ~(int64_t)15; }
+
 extern "C" int64_t paradmm_noalloc_state_bytes(int n_circles, int n_walls)
 {
     if (n_circles < 2 || n_circles > NA_MAX_CIRCLES || n_walls < 0 || n_walls > NA_MAX_WALLS) return -1;
     return na_tiles_of(n_circles) * pk_tile_floats(NA_BW) * 4 + (int64_t)n_circles * n_walls * 2 * sizeof(float4) +
-           (int64_t)n_circles * sizeof(float2) + (int64_t)n_circles * sizeof(float4) + 16;
+           na_rad_bytes(n_circles) + (int64_t)n_circles * sizeof(float4) + 16;
 }
 
 // Per-device set-up: the scratch's device address (cudaGetSymbolAddress with
@@ -182,6 +186,8 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         return pdm_set_error(PARADMM_EINVAL, "noalloc: %d walls is outside [0, %d]", d.n_walls, NA_MAX_WALLS);
     if (!(d.rho > 0) || !(d.rho_radius > 0)) return pdm_set_error(PARADMM_EINVAL, "noalloc: penalties must be positive");
     if (sweeps < 0) return pdm_set_error(PARADMM_EINVAL, "noalloc: sweeps < 0");
+    if (((uintptr_t)d_state & 15u) || ((uintptr_t)d_circles & 7u))
+        return pdm_set_error(PARADMM_EINVAL, "noalloc: d_state must be 16-byte and d_circles 8-byte aligned");
     if (device < 0 || device >= NA_MAX_DEVICES) return pdm_set_error(PARADMM_ENODEVICE, "noalloc: bad device %d", device);
     std::lock_guard<std::mutex> lk(g_na_mu);
     int prev = -1;
@@ -231,7 +237,7 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     D.wall_X = (float4 *)((char *)d_state + tile_bytes);
     D.wall_U = D.wall_X + nwall;
     D.rad_XU = (float2 *)(D.wall_U + nwall);
-    D.Zp = (float4 *)(D.rad_XU + N);
+    D.Zp = (float4 *)((char *)D.rad_XU + na_rad_bytes(N));
     int *d_mode = (int *)(D.Zp + N);
 
     // Tables into the scratch; residual partials start at zero (the array
@@ -296,7 +302,7 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         PDM_CUDA(cudaMemcpyAsync(&s_status, D.status, sizeof s_status, cudaMemcpyDeviceToHost, s));
         PDM_CUDA(cudaStreamSynchronize(s));
         if (s_ctl.err != DEV_OK)
-            return pdm_set_error(PARADMM_ETIMEOUT, "noalloc: a grid barrier wait ran out (device error %d)", s_ctl.err);
+            return pdm_set_error(PARADMM_ETIMEOUT, "noalloc: a device-side wait ran out (%s)", pdm_dev_err_name(s_ctl.err));
         const long long last = std::min<long long>(s_status.last_iter, it0 + s_ctl.pad[0] - 1);
         const long long ran = last - it0 + 1;
         done += ran;

@@ -337,9 +337,9 @@ int paradmm_gpu_shard_finish(paradmm_gpu *h, void *stream, paradmm_stats *stats)
  * is ignored).  The caller passes, in device memory it owns:
  *   d_circles  n_circles x [cx, cy, r] doubles: the consensus, read at the
  *              start and written back at the end;
- *   d_state    paradmm_noalloc_state_bytes(n_circles, n_walls) bytes: the
- *              FP32 edge state in the engine's layout (opaque to the
- *              caller).  With init_state = 1 it is first set to the plain
+ *   d_state    paradmm_noalloc_state_bytes(n_circles, n_walls) bytes,
+ *              16-byte aligned: the FP32 edge state in the engine's layout
+ *              (opaque to the caller).  With init_state = 1 it is first set to the plain
  *              start X_e = Z_v(e), U = 0; with init_state = 0 it must hold
  *              the state a previous call left, so consecutive calls continue
  *              one solve.

@@ -35,11 +35,11 @@ def _desc(N, walls, circles):
     return d
 
 
-def test_noalloc_matches_handle_api_on_two_calls():
+@pytest.mark.parametrize("N", [300, 301])  # odd N: the state's FP32 circles still start 16-byte aligned
+def test_noalloc_matches_handle_api_on_two_calls(N):
     import torch
 
     lib = eb.load()
-    N = 300
     walls = np.ascontiguousarray(eb.box_walls(1.5, 1.0))
     circles = eb.seeded_circles(N, 1.5, 1.0, 0.05, 42)
     desc = _desc(N, walls, circles)
