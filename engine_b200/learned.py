@@ -333,17 +333,6 @@ def train_weights(n_instances: int = 20000, epochs: int = 40, seed: int = 100000
                 candidates=report, out=out)
 
 
-if __name__ == "__main__":
-    import argparse
-    import json
-    ap = argparse.ArgumentParser(description="train the set-MLP warm start on packings the plain solver produces")
-    ap.add_argument("--instances", type=int, default=20000)
-    ap.add_argument("--epochs", type=int, default=40)
-    ap.add_argument("--out", default=WEIGHTS)
-    a = ap.parse_args()
-    print(json.dumps(train_weights(a.instances, a.epochs, out=a.out)))
-
-
 def tune(instances, sweeps: int, tol: float, device: int = 0) -> dict:
     """Tile side and schedule for batches like `instances`
     (paradmm_gpu_create_packing_tuned with probe solve(sweeps, tol))."""
@@ -357,3 +346,14 @@ def tune(instances, sweeps: int, tol: float, device: int = 0) -> dict:
                                                C.byref(t)))
     lib.paradmm_gpu_destroy(p)
     return {k: getattr(t, k) for k, _ in Tuning._fields_ if k != "reserved"}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the set-MLP warm start on packings the plain solver produces")
+    ap.add_argument("--instances", type=int, default=20000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--out", default=WEIGHTS)
+    a = ap.parse_args()
+    print(json.dumps(train_weights(a.instances, a.epochs, out=a.out)))
