@@ -167,6 +167,28 @@ def test_packing_teacher_forced_containers_and_exponents(container, exponent):
     assert checked >= 2
 
 
+def test_packing_teacher_forced_every_iterate_to_2000():
+    """At every k < 2000: the reference's iterate k uploaded, one engine
+    sweep, against the reference's iterate k + 1 (one handle, re-uploaded
+    each step), through the chaotic early phase and on to convergence."""
+    N = 40
+    pg, orc, _ = problem(N, 17)
+    worst, worst_k = 0.0, -1
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
+        for k in range(2000):
+            for key, v in orc.state().items():
+                pg.G.arr(key)[:] = v
+            h.upload(pg.G)
+            h.iterate(1)
+            h.download(pg.G)
+            orc.sweep()
+            d = maxdiff(pg.G.state(), orc.state())
+            if d > worst:
+                worst, worst_k = d, k
+            assert d <= TOL_F32, f"k={k}: max diff {d}"
+    print(f"teacher-forced, every k < 2000: worst max|diff| = {worst:.3e} at k = {worst_k}")
+
+
 def test_packing_free_running_from_init():
     """Free-running from the random init.  The early phase is chaotic: an
     FP32 re-evaluation of the same formulas on the CPU leaves 1e-4 of the
