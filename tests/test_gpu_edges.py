@@ -71,21 +71,26 @@ def _radius_recurrence(r0: float, n_identity: int, sweeps: int) -> np.ndarray:
     return np.array(out)
 
 
-def test_full_size_separated_grid_follows_the_scalar_recurrence():
-    N, W, H = 8000, 2.0, 1.0
-    nx, ny = 126, 64  # 8064 grid points, spacing ~0.0159 x 0.0156
+@pytest.mark.parametrize("N,nx,ny,K", [(8000, 126, 64, 40),      # the bench's size, spacing ~0.0159 x 0.0156
+                                      (32767, 256, 128, 200)])  # the largest instance the engine takes
+def test_full_size_separated_grid_follows_the_scalar_recurrence(N, nx, ny, K):
+    """N = 32767 has 536,821,761 pair factors (2.1e9 reference edges, 12.9 GB
+    of pair state): indices beyond 2^31 in every tile and partial-sum
+    address."""
+    W, H = 2.0, 1.0
     gx, gy = np.meshgrid((np.arange(nx) + 0.5) * W / nx, (np.arange(ny) + 0.5) * H / ny, indexing="ij")
     pts = np.stack([gx.ravel(), gy.ravel()], axis=1)[:N]
     r0 = 0.002
     circles = np.concatenate([pts, np.full((N, 1), r0)], axis=1)
     d = dict(n_circles=N, walls=eb.box_walls(W, H), exponent=EXP, rho=RHO, rho_radius=RHO_R, alpha=ALPHA,
              init=circles)
-    K = 40
     want = _radius_recurrence(r0, N - 1 + 4, K)
     assert want[-1] < 0.0045  # still far from any contact: the identity-prox premise holds
+    assert (want[-1] - r0) / r0 > 100 * 1e-5  # the radii move well beyond the tolerance below
     with eb.Handle.packing([d]) as h:
-        for k in (1, 2, 10, K):
-            h.iterate(k - (0 if k == 1 else prev))
+        prev = 0
+        for k in sorted({1, 2, 10, K}):
+            assert h.solve(k - prev, -1.0)["iterations"] == k - prev
             prev = k
             c = h.circles(0, N)
             assert np.abs(c[:, :2] - pts).max() <= 1e-6, f"centres moved at sweep {k}"
