@@ -157,3 +157,56 @@ def test_two_gloo_ranks_reproduce_the_reference_consensus():
     assert [r[1] for r in res] == [40, 40] and [r[2] for r in res] == [40, 40]
     assert res[0][4] == res[1][4]  # identical consensus on both ranks
     assert max(r[3] for r in res) <= 1e-12  # the sharded sums are the reference's, up to association
+
+
+def _leaver(rank, world, port, q):
+    """Rank 1 runs 10 sweeps and exits; rank 0 asks for 40 and must get an
+    error from its next exchange, not wait for ever."""
+    import datetime
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch
+    import torch.distributed as dist
+
+    import oracle_lib as O
+    from engine_b200.shard import run_sharded
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    N = 150
+    ex = torch.zeros(4 * N, dtype=torch.float64)
+    sh = _HostShard(O, N, eb.box_walls(1.0, 1.0), rank, world, 64, ex)
+    try:
+        st = run_sharded(sh, ex, lambda t: dist.all_reduce(t), maxiter=10 if rank == 1 else 40, tol=-1.0,
+                         poll_every=5)
+        q.put((rank, "done", st["iterations"]))
+    except Exception as e:  # the failure under test, reported to the parent
+        q.put((rank, "error", sh.sweeps, type(e).__name__))
+    if rank == 1:
+        q.close()
+        q.join_thread()  # the report reaches the parent before the process vanishes
+        os._exit(0)      # leaves between sweeps, without a goodbye to the group
+    dist.destroy_process_group()
+
+
+def test_a_rank_leaving_ends_the_others_run_with_an_error():
+    import time
+
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_leaver, args=(r, 2, port, q)) for r in range(2)]
+    t0 = time.time()
+    for p in procs:
+        p.start()
+    try:
+        res = sorted(q.get(timeout=120) for _ in range(2))
+    finally:
+        for p in procs:
+            p.join(60)
+            if p.is_alive():
+                p.kill()
+    assert res[1][1:] == ("done", 10)
+    assert res[0][1] == "error" and res[0][2] == 10  # rank 0 stopped at its first exchange without the peer
+    assert time.time() - t0 < 120
