@@ -13,7 +13,7 @@ import pytest
 import torch
 
 import engine_b200 as eb
-from engine_b200.shard import Shard, run_sharded, shard_rows
+from engine_b200.shard import Shard, shard_rows
 
 pytestmark = pytest.mark.gpu
 
