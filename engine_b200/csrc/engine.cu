@@ -417,11 +417,21 @@ static int pick_V(const paradmm_gpu_opts &o, int maxN)
 
 // Allocates and uploads everything of a packing handle whose host tables
 // (inst, items, circ, walls, rads, init_Z) are filled.
-// Per-instance schedule parameters.  Large instances are the critical path
-// of a batch: the first n_coop of the order (N >= coop_min_n) get a whole
-// cluster of `cluster` CTAs each; the rest run one per CTA.  cluster 0:
-// default (2); a size the device cannot launch falls back to the next
-// smaller one.
+// Per-instance schedule parameters.  Large instances are queued first and
+// the first n_coop of the order (N >= coop_min_n) get a whole cluster of
+// `cluster` CTAs each; the rest run one per CTA, starting with the instances
+// the on-chip solver takes.  Those cost little per sweep, but any of them
+// that cycles runs every sweep of the call, so n_early clusters (enough for
+// one each) start on them at once instead of after every large instance.
+// cluster 0: default (2); a size the device cannot launch falls back to the
+// next smaller one.
+static bool pk_small_path(const PkHost &P, int i)
+{
+    const PkInst &I = P.inst[i];
+    const PkCircle &C = P.circ[I.circle_base];
+    return I.N <= PK_SMALL_N && I.nb == 1 && C.wall_count <= PK_SMALL_W && C.rad_count == 1;
+}
+
 static void pk_set_instance_schedule(paradmm_gpu *h, int cluster, int coop_min_n)
 {
     PkHost &P = *h->pk;
@@ -437,9 +447,23 @@ static void pk_set_instance_schedule(paradmm_gpu *h, int cluster, int coop_min_n
     if (pk_instances_blocks_per_sm(P.V, P.stream_hint, &ib) != cudaSuccess || ib < 1) ib = 1;
     P.inst_grid = cl > 1 ? nclu * cl : h->num_sms * ib;
     P.coop_min_n = coop_min_n > 0 ? coop_min_n : 200;
+    std::vector<int> by_n(P.n_inst);
+    for (int i = 0; i < P.n_inst; ++i) by_n[i] = i;
+    std::stable_sort(by_n.begin(), by_n.end(), [&](int a, int b) { return P.inst[a].N > P.inst[b].N; });
     P.n_coop = 0;
     if (cl > 1)
-        for (int q = 0; q < P.n_inst && P.inst[P.order[q]].N >= P.coop_min_n; ++q) P.n_coop = q + 1;
+        for (int q = 0; q < P.n_inst && P.inst[by_n[q]].N >= P.coop_min_n; ++q) P.n_coop = q + 1;
+    P.order.assign(by_n.begin(), by_n.begin() + P.n_coop);
+    int n_small = 0;
+    for (int q = P.n_coop; q < P.n_inst; ++q)
+        if (pk_small_path(P, by_n[q])) { P.order.push_back(by_n[q]); ++n_small; }
+    for (int q = P.n_coop; q < P.n_inst; ++q)
+        if (!pk_small_path(P, by_n[q])) P.order.push_back(by_n[q]);
+    P.n_early = 0;
+    if (cl > 1 && P.n_coop > 0 && n_small > 0)
+        P.n_early = std::min((n_small + cl - 1) / cl, P.inst_grid / cl / 8);  // at most 1/8 of the clusters
+    if (P.d_order && cudaMemcpy(P.d_order, P.order.data(), sizeof(int) * P.n_inst, cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaGetLastError();  // the queue keeps its previous order; still a valid permutation
 }
 
 static int pk_finalize_build(paradmm_gpu *h)
@@ -874,7 +898,7 @@ static int pk_enqueue_instances(paradmm_gpu *h, const PkRun &R, bool capturing)
     PDM_CUDA(cudaMemcpyAsync(P.D.status, P.h_status, sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
     PDM_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(DevCtl), h->stream));
     PDM_CUDA(cudaEventRecordWithFlags(h->ev0, h->stream, evflags));
-    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, &h->ctl->item_ctr[0],
+    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, P.n_early, &h->ctl->item_ctr[0],
                                         P.inst_grid, P.cluster, h->stream);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "per-instance packing launch", __FILE__, __LINE__);
     PDM_CUDA(cudaEventRecordWithFlags(h->ev1, h->stream, evflags));
@@ -925,6 +949,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     key.prof = R.prof;
     key.cluster = P.cluster;
     key.n_coop = P.n_coop;
+    key.n_early = P.n_early;
     key.inst_grid = P.inst_grid;
     if (P.use_graphs && (!P.graph_exec || memcmp(&key, &P.graph_key, sizeof key) != 0)) {
         pk_drop_graph(P);

@@ -31,7 +31,7 @@ struct GraphInfo {
 struct PkGraphKey {
     int n_iter;
     double tol;
-    int check_every, fallback_after, prof, cluster, n_coop, inst_grid;
+    int check_every, fallback_after, prof, cluster, n_coop, inst_grid, n_early;
 };
 
 struct PkHost {
@@ -64,6 +64,7 @@ struct PkHost {
     int cluster = 1;                 // CTAs per large instance in the per-instance schedule
     int coop_min_n = 0;              // instances with N >= this are solved by a whole cluster
     int n_coop = 0;                  // how many instances that is (the first n_coop of the order)
+    int n_early = 0;                 // clusters that start on the on-chip-solver instances (after the coop part of the order)
     std::vector<int> order;          // instances, largest first (per-instance schedule)
     int *d_order = nullptr;          // the same on the device
     int prof = 0;                    // per-phase timing requested

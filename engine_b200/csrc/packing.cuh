@@ -53,6 +53,10 @@
 #include "common.cuh"
 
 #define PK_THREADS 256
+// The per-instance schedule's on-chip solver takes instances of at most
+// PK_SMALL_N circles (one tile) with at most PK_SMALL_W walls per circle.
+#define PK_SMALL_N 40
+#define PK_SMALL_W 4
 #define PK_WARPS (PK_THREADS / 32)
 #define PK_COMPS 6
 

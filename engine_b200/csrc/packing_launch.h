@@ -8,7 +8,7 @@
 cudaError_t pk_launch_persistent(int V, bool stream_hint, const PkDev &D, const PkRun &R, int grid, cudaStream_t s);
 cudaError_t pk_max_blocks_per_sm(int V, bool stream_hint, int *blocks);
 cudaError_t pk_launch_instances(int V, bool stream_hint, const PkDev &D, const PkRun &R, const int *order, int n_coop,
-                                unsigned *queue, int grid, int cluster, cudaStream_t s);
+                                int n_early, unsigned *queue, int grid, int cluster, cudaStream_t s);
 cudaError_t pk_instances_max_clusters(int V, bool stream_hint, int cluster, int *clusters);
 cudaError_t pk_instances_blocks_per_sm(int V, bool stream_hint, int *blocks);
 cudaError_t pk_launch_init(int V, const PkDev &D, int inst, const float *pair_duals, int grid, cudaStream_t s,
