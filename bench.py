@@ -287,6 +287,35 @@ def run_ttr(local: int):
             "max_violation_learned": max(float(x["max_violation"]) for x in le["stats"])}
 
 
+E2E_HOST_BYTES = 15e9  # one rank's host graph of the workload (X, M, N, U, RHOS, ALPHAS, edge lists)
+
+
+def host_mem_available():
+    """Bytes this process may still allocate: MemAvailable, capped by a
+    cgroup memory limit when one is set (None if neither can be read)."""
+    vals = []
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    vals.append(int(line.split()[1]) * 1024)
+    except OSError:
+        pass
+    for lim, cur in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                     ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            with open(lim) as f:
+                l = f.read().strip()
+            with open(cur) as f:
+                c = int(f.read().strip())
+            if l != "max" and int(l) < (1 << 60):
+                vals.append(int(l) - c)
+            break
+        except (OSError, ValueError):
+            continue
+    return min(vals) if vals else None
+
+
 def run_e2e(args, local: int):
     """updateGOpenMP(G, sweeps, threads) on a host graph of the workload."""
     import engine_b200 as eb
@@ -349,12 +378,30 @@ def run_engine_arm(args):
     traffic_sweep = profiled_traffic()
     e2e = None
     if not args.no_e2e and n == N_CIRCLES:
-        try:
-            e2e = run_e2e(args, local)
-            e2e_v = allreduce_max(world, -e2e["value"])  # slowest rank sets the aggregate
-            e2e["value"] = world * (-e2e_v)
-        except Exception as ex:  # report, never fake
-            e2e = {"value": None, "unit": METRIC, "error": str(ex)[:200]}
+        # every rank builds its own FP64 host graph (about 15 GB at N = 8000,
+        # page-locked for the copies): skip the leg on all ranks alike rather
+        # than drive the host out of memory
+        ranks_here = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+        need = E2E_HOST_BYTES * ranks_here
+        avail = host_mem_available()
+        short = avail is not None and avail < 1.25 * need
+        if allreduce_max(world, 1.0 if short else 0.0) > 0:
+            e2e = {"value": None, "unit": METRIC,
+                   "skipped": f"host memory: {ranks_here} host graphs need about {need / 1e9:.0f} GB, "
+                              f"{(avail or 0) / 1e9:.0f} GB available"}
+        else:
+            rate, err = None, None
+            try:
+                e2e = run_e2e(args, local)
+                rate = e2e["value"]
+            except Exception as ex:  # report, never fake
+                err = str(ex)[:200]
+            # the slowest rank sets the aggregate; every rank takes part, a failed one as +inf
+            worst = allreduce_max(world, -rate if rate is not None else float("inf"))
+            if err is not None or worst == float("inf"):
+                e2e = {"value": None, "unit": METRIC, "error": err or "the end-to-end leg failed on another rank"}
+            else:
+                e2e["value"] = world * (-worst)
     ttr = None
     if world == 1 and not args.no_ttr and n == N_CIRCLES:
         try:
