@@ -396,23 +396,11 @@ class Handle:
     def packing(cls, descs: list[dict], **kw) -> "Handle":
         """descs: dicts with n_circles, walls (k x 4), exponent, rho, rho_radius, alpha, init (N x 3)."""
         lib = load()
-        arr = (PackingDesc * len(descs))()
-        keep = []
-        for i, d in enumerate(descs):
-            walls = np.ascontiguousarray(d["walls"], dtype=np.float64)
-            init = np.ascontiguousarray(d["init"], dtype=np.float64)
-            keep += [walls, init]
-            arr[i].n_circles = int(d["n_circles"])
-            arr[i].n_walls = int(walls.shape[0])
-            arr[i].walls = walls.ctypes.data_as(C.POINTER(C.c_double))
-            arr[i].exponent = float(d.get("exponent", 2.0))
-            arr[i].rho = float(d["rho"])
-            arr[i].rho_radius = float(d["rho_radius"])
-            arr[i].alpha = float(d["alpha"])
-            arr[i].init = init.ctypes.data_as(C.POINTER(C.c_double))
+        arr, keep = cls._descs(descs)  # keep: the arrays arr points into, alive until the call returns
         p = C.c_void_p()
         o = opts(**kw)
         check(lib.paradmm_gpu_create_packing(arr, len(descs), C.byref(o), C.byref(p)))
+        del keep
         return cls(p.value, lib)
 
     def iterate(self, n: int) -> None:
