@@ -61,3 +61,13 @@ def test_reference_arm_prints_once_under_torchrun():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["cores"] >= 1
+
+
+def test_host_memory_probe_for_the_end_to_end_leg():
+    """bench.py sizes the e2e leg's host graphs against this (bytes the
+    process may still allocate; a cgroup limit caps MemAvailable)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    avail = bench.host_mem_available()
+    assert avail is None or avail > 0
+    assert bench.E2E_HOST_BYTES >= 13.6e9  # measured peak resident size of one N = 8000 host graph
