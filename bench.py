@@ -16,14 +16,20 @@ Arms:
                     resident); `e2e` is the same metric through the drop-in
                     paradmm.h call updateGOpenMP(G, sweeps, threads) on a host
                     graph, with its uploads and downloads in the timed region.
+                    `cpu_baseline` is the reference's updateGOpenMP on the
+                    same N = 8000 graph, 10 sweeps, all host cores.
   --impl reference  the reference's own CPU path (updateGOpenMP of
                     core/paradmm.c, compiled from its sources into oracle/_ref
-                    with its -Ofast flags) on all host cores, on a bounded
-                    sample of the workload.
+                    with its -Ofast flags) on all host cores, on the same
+                    N = 8000 graph: W warm-up sweeps, then K timed sweeps
+                    (fewer only when K sweeps would exceed REF_BUDGET_S; the
+                    line says how many ran).
 
-Also reported (single GPU): time_to_residual, the batched workload (512
-instances, N in [20, 400]) solved to r + s <= 1e-5 from the plain start and
-from the set-MLP warm start (inference included), host wall clock.
+Also reported: time_to_residual, the batched workload (512 instances, N in
+[20, 400]) solved to r + s <= 1e-5 from the plain start and from the set-MLP
+warm start (inference included), host wall clock; with N GPUs the instances
+are dealt over the ranks (no communication) and the time is the slowest
+rank's.
 
 Multi-GPU (torchrun, one process per GPU): every rank solves its own
 instance (replicas, weak scaling; the path has no cross-instance exchange);
@@ -38,9 +44,7 @@ import ctypes as C
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -50,6 +54,15 @@ METRIC = "edge-updates/s"
 N_CIRCLES, BOX_W, BOX_H, RMAX, SEED = 8000, 2.0, 1.0, 0.01, 20261203
 RHO, RHO_R, ALPHA, EXPONENT = 10.0, 5.0, 1.0, 2.0
 N_WALLS = 4
+CPU_SWEEPS = 10         # cpu_baseline leg: sweeps of the reference on the full graph
+REF_BUDGET_S = 150.0    # reference arm: cap on the timed sweeps' CPU time
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of ONE pk_persistent
+# launch of NCU_SWEEPS sweeps of this workload (N = 8000, bench seed), from one
+# ncu capture of `bench.py --steps 20 --warmup 3 --no-e2e --no-ttr --no-cpu`;
+# profiles/pk_persistent_n8000_dram.md has the command and the figures.
+NCU_DRAM_BYTES_N8000 = None
+NCU_SWEEPS = 20
 
 
 def edges_of(n: int) -> int:
@@ -72,49 +85,77 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per sweep from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "pk_persistent_n4000_full.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("dram_bytes_per_sweep:"):
-            return float(line.split(":", 1)[1].split()[0])
-    return None
-
-
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons."""
+    """SM clock and throttle reasons sampled through NVML (the data
+    nvidia-smi reports) by a thread that polls as fast as NVML answers,
+    started before the timed region.  `stop(t0, t1)` keeps the samples whose
+    host timestamps fall inside [t0, t1], the timed region; when that region
+    holds fewer than three samples it adds the last sample before and the
+    first after it, and says so."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+            ("sw_power_cap", 0x4))
 
-    def __init__(self, gpus: str):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    def __init__(self, devices: list[int]):
+        import threading
+        self.rows: list[tuple] = []
+        self.err = None
+        self.run = False
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", gpus, f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = []
+            for d in devices:
+                try:
+                    uuid = str(torch.cuda.get_device_properties(d).uuid)
+                    self.h.append(pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid))
+                except Exception:
+                    self.h.append(pynvml.nvmlDeviceGetHandleByIndex(d))
+        except Exception as ex:  # report, never fake
+            self.err = f"NVML unavailable: {str(ex)[:80]}"
+            return
+        self.run = True
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
+        time.sleep(0.01)
 
-    def stop(self) -> dict:
-        if self.p is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.p.terminate()
+    def _poll(self):
+        nv = self.nv
+        while self.run:
+            for h in self.h:
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((time.perf_counter(), sm, mx, rs))
+                    time.sleep(0.0002)
+                except Exception as ex:
+                    self.err = str(ex)[:80]
+                    self.run = False
+
+    def stop(self, t0: float, t1: float) -> dict:
+        if not self.run and not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "no samples"], "samples": 0}
+        self.run = False
+        self.t.join(timeout=5)
         try:
-            self.p.wait(timeout=5)
+            self.nv.nvmlShutdown()
         except Exception:
-            self.p.kill()
-        self.f.flush()
-        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.count(",") >= 8]
-        os.unlink(self.f.name)
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+            pass
+        rows = sorted(self.rows)
+        inside = [r for r in rows if t0 <= r[0] <= t1]
+        note = "samples inside the timed region"
+        if len(inside) < 3:
+            inside = [r for r in rows if r[0] < t0][-1:] + inside + [r for r in rows if r[0] > t1][:1]
+            note = "timed region holds fewer than three NVML samples: the samples just before and after it added"
+        sm = [r[1] for r in inside]
+        reasons = sorted({n for r in inside for n, b in self.BITS if r[3] & b})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(r[2] for r in inside) if inside else None,
+                "reasons": reasons, "samples": len(inside), "source": "NVML", "note": note,
+                "timed_region_ms": round((t1 - t0) * 1e3, 3)}
 
 
 def dist_init():
@@ -180,57 +221,50 @@ def reference_lib():
     return oracle_lib._load(oracle_lib.PORT), "port"
 
 
-def reference_rate(n: int, sweeps: int, threads: int):
-    """Edge-updates/s of the reference's updateGOpenMP on an n-circle sample of
-    the workload (same box, radii and penalties)."""
+def reference_run(n: int, warmup: int, sweeps: int, threads: int, budget_s: float | None = None) -> dict:
+    """The reference's updateGOpenMP on the workload's graph with n circles
+    (same box, radii, penalties and seeded start as the engine arm's rank 0):
+    `warmup` untimed sweeps, then `sweeps` timed ones in one call -- fewer
+    when budget_s is given and the warm-up rate says they would take longer
+    (at least one)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
 
     import engine_b200 as eb
     lib, kind = reference_lib()
+    t = time.time()
     P = oracle_lib.OraclePacking(lib, n, eb.box_walls(BOX_W, BOX_H), EXPONENT)
     P.init(SEED, BOX_W, BOX_H, RMAX, RHO, RHO_R, ALPHA)
-    dt = lib.orc_time_sweeps(P.graph_ptr(), sweeps, threads)
+    build_s = time.time() - t
+    run = sweeps
+    if warmup:
+        wt = lib.orc_time_sweeps(P.graph_ptr(), warmup, threads)
+        if budget_s is not None:
+            run = max(1, min(sweeps, int(budget_s / (wt / warmup))))
+    dt = lib.orc_time_sweeps(P.graph_ptr(), run, threads)
     E = P.G.num_edges
     P.close()
-    return E * sweeps / dt, dt, E, kind
-
-
-def cpu_sample_size(threads: int, budget_s: float, sweeps: int) -> int:
-    rate, _, _, _ = reference_rate(400, 2, threads)
-    n = int((rate * budget_s / sweeps / 2.0) ** 0.5)
-    return max(200, min(n, 4000))
+    return {"rate": E * run / dt, "seconds": dt, "edges": E, "kind": kind, "sweeps": run, "build_s": build_s}
 
 
 def run_reference_arm(args):
-    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    per_step = min(1.0, 150.0 / max(1, args.steps + args.warmup))
-    n = cpu_sample_size(threads, per_step, 1)
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib
-
-    import engine_b200 as eb
-    lib, kind = reference_lib()
-    P = oracle_lib.OraclePacking(lib, n, eb.box_walls(BOX_W, BOX_H), EXPONENT)
-    P.init(SEED, BOX_W, BOX_H, RMAX, RHO, RHO_R, ALPHA)
-    if args.warmup:
-        lib.orc_time_sweeps(P.graph_ptr(), args.warmup, threads)
-    dt = lib.orc_time_sweeps(P.graph_ptr(), args.steps, threads)
-    E = P.G.num_edges
-    rate = E * args.steps / dt
-    sample = (f"N={n} circles of the workload's distribution ({E} edges), {args.steps} sweeps of "
-              f"updateGOpenMP, {threads} threads")
+    n = args.circles
+    r = reference_run(n, args.warmup, args.steps, threads, REF_BUDGET_S)
+    sample = (f"the full N={n} graph ({r['edges']} edges), {args.warmup} warm-up + {r['sweeps']} timed sweeps of "
+              f"updateGOpenMP in one call, {threads} threads (nproc {os.cpu_count()})")
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"plain circle packing N={N_CIRCLES}, {BOX_W:g}x{BOX_H:g} box (CPU leg: bounded sample)",
-                   "sample_circles": n, "sample_edges": E},
-        "cpu_baseline": {"value": rate, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample},
-        "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": METRIC, "value": r["rate"], "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / r["sweeps"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"plain circle packing N={n}, {BOX_W:g}x{BOX_H:g} box, radii in [0,{RMAX}], "
+                               f"seeded uniform init", "circles": n, "edges": r["edges"],
+                   "timed_sweeps": r["sweeps"], "graph_build_s": round(r["build_s"], 2)},
+        "cpu_baseline": {"value": r["rate"], "unit": METRIC, "cores": threads, "kind": r["kind"], "sample": sample},
+        "e2e": {"value": r["rate"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
 
@@ -242,49 +276,73 @@ def run_reference_arm(args):
 TTR_INSTANCES, TTR_SEED, TTR_MAXITER, TTR_TOL, TTR_BUDGET = 512, 900000, 20000, 1e-5, 0
 
 
-def run_ttr(local: int):
+def run_ttr(local: int, world: int = 1, rank: int = 0):
     """Time to residual on the batched workload: 512 instances (N uniform in
     [20, 400], box aspect uniform in [1, 2]), host wall clock from the solve
     call until every instance has r + s <= 1e-5 or used its iteration cap.
     plain: the batch handle's plain start.  learned: set-MLP features and
     forward, warm start, then one solve (TTR_BUDGET > 0 would restart
     instances not converged after that many sweeps from their plain start in
-    the same launch).  Both run once untimed first, on
-    the schedule the autotuner picked for batches of this distribution."""
+    the same launch).  Both run once untimed first, on the schedule the
+    autotuner picked for batches of this distribution.  With world > 1 rank r
+    solves its share of the instances (engine_b200.shard.split_instances; no
+    communication); each arm's time is the slowest rank's and rank 0 gathers
+    the per-instance results."""
     import numpy as np
 
     from engine_b200 import learned
-    inst = learned.make_instances(TTR_INSTANCES, TTR_SEED)
+    from engine_b200.shard import gather_instances, split_instances
+    inst_all = learned.make_instances(TTR_INSTANCES, TTR_SEED)
+    mine = split_instances([d["n_circles"] for d in inst_all], world, rank)
+    inst = [inst_all[i] for i in mine]
     # schedule from the autotuner, tuned on another seeded batch of the same
     # distribution (probe = full solves to the tolerance; untimed, like
     # creating the handle), used by both arms
-    tune = learned.tune(learned.make_instances(TTR_INSTANCES, TTR_SEED + 1), TTR_MAXITER, TTR_TOL, device=local)
+    tune_all = learned.make_instances(TTR_INSTANCES, TTR_SEED + 1)
+    tune = learned.tune([tune_all[i] for i in split_instances([d["n_circles"] for d in tune_all], world, rank)],
+                        TTR_MAXITER, TTR_TOL, device=local)
     kw = dict(schedule=tune["schedule"], cluster=tune["cluster_size"], coop_min_n=tune["coop_min_n"],
               block_width=tune["block_width"])
     net = learned.SetMLP(device=local)
     net.load()
     for _ in range(2):
+        barrier(world)
         pl = learned.solve_plain(inst, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local, **kw)
+        barrier(world)
         le = learned.solve_learned(inst, net, budget=TTR_BUDGET, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local, **kw)
     net.close()
-    tot_p = sum(float(c[:, 2].sum()) for c in pl["circles"])
-    tot_l = sum(float(c[:, 2].sum()) for c in le["circles"])
-    its_p = np.array([x["iterations"] for x in pl["stats"]])
-    its_l = np.array([x["iterations"] for x in le["stats"]])
+    plain_s = allreduce_max(world, pl["wall_s"])
+    learned_s = allreduce_max(world, le["wall_s"])
+
+    def rows(res):
+        return [(s["iterations"], int(s["converged"]), float(s["max_violation"]), float(c[:, 2].sum()),
+                 int(s.get("fallback", 0))) for s, c in zip(res["stats"], res["circles"])]
+
+    P = gather_instances(mine, rows(pl), TTR_INSTANCES, world)
+    L = gather_instances(mine, rows(le), TTR_INSTANCES, world)
+    if rank != 0:
+        return None
+    its_p = np.array([x[0] for x in P])
+    its_l = np.array([x[0] for x in L])
+    tot_p = sum(x[3] for x in P)
+    tot_l = sum(x[3] for x in L)
     return {"workload": f"{TTR_INSTANCES} packing instances, N uniform in [20,400], aspect uniform in [1,2], "
                         f"seeded Gaussian-code plain starts (seed {TTR_SEED})",
             "tol": TTR_TOL, "maxiter": TTR_MAXITER, "learned_budget": TTR_BUDGET,
+            "ranks": world, "split": "instances dealt over the ranks by size (snake order), no communication",
             "schedule": {"schedule": "instance" if tune["schedule"] == 2 else "grid", "block_width": tune["block_width"],
                          "cluster": tune["cluster_size"],
                          "coop_min_n": tune["coop_min_n"], "autotune_candidates": tune["candidates"],
                          "probe_ms_best": tune["ms"], "probe_ms_worst": tune["worst_ms"]},
-            "plain_s": pl["wall_s"], "learned_s": le["wall_s"], "speedup": pl["wall_s"] / le["wall_s"],
-            "converged_plain": int(sum(x["converged"] for x in pl["stats"])),
-            "converged_learned": int(sum(x["converged"] for x in le["stats"])),
-            "fallbacks": le["fallbacks"],
+            "plain_s": plain_s, "learned_s": learned_s, "speedup": plain_s / learned_s,
+            "converged_plain": int(sum(x[1] for x in P)), "converged_learned": int(sum(x[1] for x in L)),
+            "fallbacks": int(sum(x[4] for x in L)),
             "median_sweeps_plain": int(np.median(its_p)), "median_sweeps_learned": int(np.median(its_l)),
+            "sweeps_quantiles_plain": [int(q) for q in np.quantile(its_p, [0.1, 0.5, 0.9, 0.99, 1.0])],
+            "sweeps_quantiles_learned": [int(q) for q in np.quantile(its_l, [0.1, 0.5, 0.9, 0.99, 1.0])],
+            "total_radius_plain": tot_p, "total_radius_learned": tot_l,
             "total_radius_rel_diff": (tot_l - tot_p) / tot_p,
-            "max_violation_learned": max(float(x["max_violation"]) for x in le["stats"])}
+            "max_violation_plain": max(x[2] for x in P), "max_violation_learned": max(x[2] for x in L)}
 
 
 E2E_HOST_BYTES = 15e9  # one rank's host graph of the workload (X, M, N, U, RHOS, ALPHAS, edge lists)
@@ -348,8 +406,6 @@ def run_e2e(args, local: int):
 
 
 def run_engine_arm(args):
-    import numpy as np
-
     import engine_b200 as eb
     world, rank, local = dist_init()
     n = args.circles
@@ -359,14 +415,15 @@ def run_engine_arm(args):
     h.iterate(max(3, args.warmup))
     E = edges_of(n)
     barrier(world)
-    clocks = Clocks(str(local) if world == 1 else ",".join(str(i) for i in range(world))) if rank == 0 else None
+    clocks = Clocks([local] if world == 1 else list(range(world))) if rank == 0 else None
     l0 = h.launches()
     t = time.perf_counter()
     s = h.solve(args.steps, -1.0)
-    wall = time.perf_counter() - t
+    t_end = time.perf_counter()
+    wall = t_end - t
     launches = h.launches() - l0
     barrier(world)
-    ck = clocks.stop() if clocks else None
+    ck = clocks.stop(t, t_end) if clocks else None
     dev_ms = allreduce_max(world, float(s["device_ms"]))
     st = h.instance_stats()[0]
     value = world * E * args.steps / (dev_ms * 1e-3)
@@ -375,7 +432,9 @@ def run_engine_arm(args):
     sweeps_per_launch = args.steps / max(1, launches)
     achieved = algo * sweeps_per_launch / (launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
-    traffic_sweep = profiled_traffic()
+    traffic = None
+    if NCU_DRAM_BYTES_N8000 is not None and n == N_CIRCLES:
+        traffic = NCU_DRAM_BYTES_N8000 / NCU_SWEEPS * sweeps_per_launch
     e2e = None
     if not args.no_e2e and n == N_CIRCLES:
         # every rank builds its own FP64 host graph (about 15 GB at N = 8000,
@@ -403,19 +462,18 @@ def run_engine_arm(args):
             else:
                 e2e["value"] = world * (-worst)
     ttr = None
-    if world == 1 and not args.no_ttr and n == N_CIRCLES:
+    if not args.no_ttr and n == N_CIRCLES:
         try:
-            ttr = run_ttr(local)
+            ttr = run_ttr(local, world, rank)
         except Exception as ex:  # report, never fake
             ttr = {"error": str(ex)[:200]}
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and n == N_CIRCLES:
+    if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        nsamp = cpu_sample_size(threads, 12.0, 10)
-        rate, dt, Es, kind = reference_rate(nsamp, 10, threads)
-        cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": kind,
-               "sample": f"N={nsamp} circles of the workload's distribution ({Es} edges), 10 sweeps of the "
-                         f"reference updateGOpenMP ({dt:.1f} s)"}
+        r = reference_run(n, 1, CPU_SWEEPS, threads)
+        cpu = {"value": r["rate"], "unit": METRIC, "cores": threads, "kind": r["kind"],
+               "sample": f"the same N={n} graph ({r['edges']} edges), 1 warm-up + {r['sweeps']} timed sweeps of "
+                         f"the reference updateGOpenMP ({r['seconds']:.1f} s), nproc {os.cpu_count()}"}
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -432,7 +490,10 @@ def run_engine_arm(args):
             "iterations_per_s": world * args.steps / (dev_ms * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": None if traffic_sweep is None else traffic_sweep * sweeps_per_launch,
+                         "traffic": traffic,
+                         "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one {NCU_SWEEPS}-sweep "
+                                            f"launch at N={N_CIRCLES}, scaled to {sweeps_per_launch:g} sweeps")
+                         if traffic is not None else None,
                          "algorithmic_bytes_per_sweep": algo, "sweeps_per_launch": sweeps_per_launch,
                          "algorithmic_bytes": "48 B per pair factor (U of 6 live components, read + written; "
                                               "X recomputed), 48 B per wall factor, 16 B per radius factor",
@@ -476,16 +537,18 @@ def run_shard_arm(args):
 
     run_sharded(sh, ex, allreduce, max(3, args.warmup), -1.0, poll_every=64)
     barrier(world)
-    clocks = Clocks(str(local) if world == 1 else ",".join(str(i) for i in range(world))) if rank == 0 else None
+    clocks = Clocks([local] if world == 1 else list(range(world))) if rank == 0 else None
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = sh.launches()
+    t = time.perf_counter()
     e0.record()
     st = run_sharded(sh, ex, allreduce, args.steps, -1.0, poll_every=max(64, args.steps))
     e1.record()
     torch.cuda.synchronize()
+    t_end = time.perf_counter()
     launches = sh.launches() - l0
     barrier(world)
-    ck = clocks.stop() if clocks else None
+    ck = clocks.stop(t, t_end) if clocks else None
     dev_ms = allreduce_max(world, e0.elapsed_time(e1))
     E = edges_of(n)
     algo = algo_bytes_per_sweep(n)
@@ -521,7 +584,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--block-width", type=int, default=0)
     ap.add_argument("--circles", type=int, default=N_CIRCLES,
-                    help="instance size (default: the benchmark workload; smaller only for profiling captures)")
+                    help="instance size (default: the benchmark workload; smaller only for profiling and tests)")
     ap.add_argument("--e2e-sweeps", type=int, default=500)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")

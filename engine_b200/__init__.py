@@ -144,11 +144,15 @@ _SIGS = {
     "paradmm_gpu_instance_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "paradmm_gpu_get_circles": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
     "paradmm_gpu_warm_start": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+    "paradmm_gpu_warm_start_duals": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                               C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]),
     "paradmm_gpu_device_bytes": (C.c_int64, [C.c_void_p]),
     "paradmm_gpu_launches": (C.c_int64, [C.c_void_p]),
     "paradmm_gpu_instance_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "paradmm_gpu_set_fallback": (C.c_int, [C.c_void_p, C.c_int64]),
+    "paradmm_gpu_set_rho_balance": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
+    "paradmm_gpu_rho_scale": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "paradmm_gpu_selftest_barrier_timeout": (C.c_int, [C.c_int, C.c_int]),
     "paradmm_gpu_register_op_source": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
     "paradmm_gpu_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
@@ -444,6 +448,20 @@ class Handle:
         check(self.lib.paradmm_gpu_warm_start(self.ptr, instance, c.ctypes.data_as(C.POINTER(C.c_double)),
                                               None if du is None else du.ctypes.data_as(C.POINTER(C.c_float))))
 
+    def warm_start_duals(self, instance: int, circles: np.ndarray, pair_duals=None, wall_duals=None,
+                         radius_duals=None, dual_iters: int = 0) -> None:
+        """paradmm_gpu_warm_start_duals: Z = circles, X = Z, U from the given
+        duals (None = 0), then dual_iters rounds of the reference's
+        optimal-initialisation map."""
+        def p(a):
+            if a is None:
+                return None, None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            return a, a.ctypes.data_as(C.POINTER(C.c_double))
+        keep = [p(circles), p(pair_duals), p(wall_duals), p(radius_duals)]
+        check(self.lib.paradmm_gpu_warm_start_duals(self.ptr, instance, keep[0][1], keep[1][1], keep[2][1], keep[3][1],
+                                                    int(dual_iters)))
+
     def engine(self) -> int:
         return self.lib.paradmm_gpu_engine(self.ptr)
 
@@ -464,6 +482,17 @@ class Handle:
 
     def set_profiling(self, on: bool) -> None:
         check(self.lib.paradmm_gpu_set_profiling(self.ptr, 1 if on else 0))
+
+    def set_rho_balance(self, period: int, mu: float = 10.0, log2_min: int = -1, log2_max: int = 4) -> None:
+        """paradmm_gpu_set_rho_balance: residual balancing of the penalties
+        every `period` iterates (0: off)."""
+        check(self.lib.paradmm_gpu_set_rho_balance(self.ptr, int(period), float(mu), int(log2_min), int(log2_max)))
+
+    def rho_scale(self, instance: int = 0) -> int:
+        """log2 of the penalty scale of the instance's next sweep."""
+        v = C.c_int()
+        check(self.lib.paradmm_gpu_rho_scale(self.ptr, int(instance), C.byref(v)))
+        return v.value
 
     def set_fallback(self, after_sweeps: int) -> None:
         """Per-instance schedule: restart unconverged instances from their plain

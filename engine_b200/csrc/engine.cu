@@ -577,42 +577,65 @@ static int pk_finalize_build(paradmm_gpu *h)
         pk_set_instance_schedule(h, h->opts.cluster_size, h->opts.reserved[0]);
     }
     P.upload_iter.assign(P.n_inst, 0);
+    P.age.assign(P.n_inst, 0);
+    P.last_swept.assign(P.n_inst, -1);
     P.nmode.assign(P.n_inst, PK_MODE_Z);
     P.status.assign(P.n_inst, PkStatus{});
-    for (auto &s : P.status) { s.resid_iter = -1; s.primal = s.dual = NAN; }
+    for (auto &s : P.status) { s.resid_iter = -1; s.primal = s.dual = NAN; pk_bal_reset(s, 0); }
     P.iters_last_call.assign(P.n_inst, 0);
     return PARADMM_OK;
 }
 
+// Instance i's state was just set (create, warm start, upload): balancing
+// ages restart, the penalty scale returns to 1.
+static void pk_state_set(PkHost &P, int i)
+{
+    P.age[i] = 0;
+    P.last_swept[i] = -1;
+    pk_bal_reset(P.status[i], 0);
+}
+
 // Plain/warm state of every instance from its Z: one launch over all
-// instances (grid.y = instance) when the grid allows it.
-static int pk_init_all(paradmm_gpu *h, int radius_duals)
+// instances (grid.y = instance) when the grid allows it.  Pair and wall duals
+// start at 0, radius duals at 0 or (radius_duals) at the radius prox's fixed
+// point; dual_iters > 0 refines them by the reference's optimal-initialisation
+// map (pk_init_state).
+static int pk_init_all(paradmm_gpu *h, int radius_duals, int dual_iters = 0)
 {
     PkHost &P = *h->pk;
     long long slots = 0;
     for (int i = 0; i < P.n_inst; ++i) slots = std::max(slots, (long long)P.inst[i].nb * (P.inst[i].nb + 1) / 2 * P.BW * P.BW);
     const int grid = (int)std::max(1LL, std::min<long long>(h->num_sms * 4, slots / 256 + 1));
+    PkInitArgs A{};
+    A.radius_duals = radius_duals;
+    A.dual_iters = dual_iters;
+    A.row_lo = P.row_lo;
+    A.row_hi = P.row_hi;
     for (int i = 0; i < P.n_inst; ++i) {
         if (P.n_inst > 65535 || i == 0) {
-            cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, nullptr, grid, h->stream, radius_duals,
-                                           P.row_lo, P.row_hi);
+            cudaError_t e = pk_launch_init(P.V, P.D, P.n_inst > 65535 ? i : -1, A, grid, h->stream);
             if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
         }
         P.nmode[i] = PK_MODE_Z;
         P.upload_iter[i] = P.it_next;
+        pk_state_set(P, i);
     }
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     return PARADMM_OK;
 }
 
-static int pk_init_instance_state(paradmm_gpu *h, int inst, const float *d_pair_duals)
+static int pk_init_instance_state(paradmm_gpu *h, int inst, const PkInitArgs &A)
 {
     PkHost &P = *h->pk;
-    cudaError_t e = pk_launch_init(P.V, P.D, inst, d_pair_duals, h->num_sms * 4, h->stream, 0, P.row_lo, P.row_hi);
+    PkInitArgs a = A;
+    a.row_lo = P.row_lo;
+    a.row_hi = P.row_hi;
+    cudaError_t e = pk_launch_init(P.V, P.D, inst, a, h->num_sms * 4, h->stream);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_init_state", __FILE__, __LINE__);
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     P.nmode[inst] = PK_MODE_Z;
     P.upload_iter[inst] = P.it_next;
+    pk_state_set(P, inst);
     return PARADMM_OK;
 }
 
@@ -848,6 +871,7 @@ static int pk_upload_graph(paradmm_gpu *h, const graph *G)
                              "the packing engine keeps one (use PARADMM_ENGINE_GENERIC_F64)");
     P.nmode[0] = PK_MODE_N;
     P.upload_iter[0] = P.it_next;
+    pk_state_set(P, 0);
     return PARADMM_OK;
 }
 
@@ -857,9 +881,15 @@ static int pk_download_graph(paradmm_gpu *h, graph *G)
     int rc = ensure_stage(h);
     if (rc) return rc;
     const int nm = P.nmode[0];
+    // a rescale of the penalties due in the next pass belongs to the U of the
+    // last sweep (the reference form applies it right after that sweep)
+    const PkStatus &bs = P.status[0];
+    const long long next_age = P.age[0] + 1;
+    const float uf = (bs.bal_pass_age > 0 && bs.bal_pass_age == next_age && bs.bal_log2_new != bs.bal_log2_cur)
+                         ? (bs.bal_log2_new > bs.bal_log2_cur ? 0.5f : 2.0f) : 1.0f;
     cudaError_t e = pk_launch_gather(P.V, P.D, 0, P.d_pmap, P.n_pmap, P.d_wmap, 0, P.n_wall, P.d_rmap, 0, P.n_rad,
-                                     P.d_cmap, P.d_wcirc, P.d_rcirc, nm, h->d_stage[0], h->d_stage[1], h->d_stage[2],
-                                     h->d_stage[3], h->d_stage[4], h->num_sms * 8, h->stream);
+                                     P.d_cmap, P.d_wcirc, P.d_rcirc, nm, uf, h->d_stage[0], h->d_stage[1],
+                                     h->d_stage[2], h->d_stage[3], h->d_stage[4], h->num_sms * 8, h->stream);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "pk_gather", __FILE__, __LINE__);
     const size_t ne = (size_t)h->num_edges * 2, nz = (size_t)h->num_vars * 2;
     double *dst[5] = {G->X, G->M, G->N, G->U, G->Z};
@@ -931,6 +961,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
         s.mode_iter = 0;
         s.pad = 0;
         s.t_begin_ns = s.t_end_ns = 0;
+        s.bal_base = -P.age[i];  // sweep 0 of this call produces the iterate of age age[i] + 1
     }
     PkRun R{};
     R.it0 = 0;
@@ -940,8 +971,16 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     R.check_every = check_every < 1 ? 1 : check_every;
     R.fallback_after = P.fallback_after < n ? P.fallback_after : 0;
     R.prof = P.prof;
+    R.bal_period = P.bal_period;
+    R.bal_mu = P.bal_mu;
+    R.bal_lmin = P.bal_lmin;
+    R.bal_lmax = P.bal_lmax;
     PkGraphKey key;
     memset(&key, 0, sizeof key);
+    key.bal_period = R.bal_period;
+    key.bal_mu = R.bal_mu;
+    key.bal_lmin = R.bal_lmin;
+    key.bal_lmax = R.bal_lmax;
     key.n_iter = R.n_iter;
     key.tol = tol;
     key.check_every = R.check_every;
@@ -994,6 +1033,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
         P.iters_last_call[i] = ran > 0 ? ran : 0;
         P.nmode[i] = pk_pending_mode(st, st.last_iter);
         P.status[i] = st;
+        P.age[i] = (ran > 0 ? ran : 0) - st.bal_base;  // a fallback restart moved bal_base
         if (st.nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
     }
     P.it_next += n;
@@ -1023,6 +1063,10 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
             s.nonfinite = 0;
             s.nmode = P.nmode[i];
             s.mode_iter = it0;
+            s.bal_base = it0 - P.age[i];
+            // the first two finalisations of a launch read residual sums of the two
+            // sweeps before it: valid only if this instance ran them
+            s.bal_eval_from = std::max(s.bal_base + 2, P.last_swept[i] == it0 - 1 ? it0 : it0 + 2);
             if (!done[i]) ++active;
         }
         if (active == 0) break;
@@ -1037,6 +1081,10 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
         R.tol = tol;
         R.check_every = check_every < 1 ? 1 : check_every;
         R.prof = P.prof;
+        R.bal_period = P.bal_period;
+        R.bal_mu = P.bal_mu;
+        R.bal_lmin = P.bal_lmin;
+        R.bal_lmax = P.bal_lmax;
         PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
         cudaError_t e = pk_launch_persistent(P.V, P.stream_hint, P.D, R, P.grid, h->stream);
         if (e != cudaSuccess) return pdm_cuda_fail(e, "packing persistent launch", __FILE__, __LINE__);
@@ -1058,6 +1106,7 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
             const long long last = std::min(st[i].last_iter, it0 + sweeps - 1);
             const long long ran = last - it0 + 1;
             if (ran > 0) P.iters_last_call[i] += ran;
+            if (ran > 0) { P.age[i] += ran; P.last_swept[i] = last; }
             P.nmode[i] = pk_pending_mode(st[i], last);
             P.status[i] = st[i];
             if (st[i].converged || st[i].nonfinite) done[i] = 1;
@@ -1192,6 +1241,11 @@ static int gen_upload(paradmm_gpu *h, const graph *G)
     PDM_CUDA(cudaMemcpyAsync((void *)D.ALPHAS, G->ALPHAS, sizeof(double) * G->num_edges, cudaMemcpyHostToDevice, h->stream));
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     Gh.zprev_valid = 0;
+    // the uploaded state starts the balancing ages; its penalties are scale 1
+    Gh.age = 0;
+    Gh.bal_log2 = 0;
+    Gh.bal_pending = 0;
+    Gh.bal_apply_age = -1;
     return PARADMM_OK;
 }
 
@@ -1264,15 +1318,38 @@ static int gen_run(paradmm_gpu *h, long long n, double tol, int check_every, par
     int converged = 0, rc = PARADMM_OK;
     double rp = NAN, rd = NAN;
     while (done < n) {
+        const long long age = Gh.age + 1;  // of the iterate this sweep produces
         const bool check = tol >= 0 && ((done + 1) % check_every == 0 || done + 1 == n);
-        if (check || done + 1 == n) {
+        const bool decide = Gh.bal_period > 0 && age % Gh.bal_period == 0;
+        if (check || decide || done + 1 == n) {
             PDM_CUDA(cudaMemcpyAsync(Gh.d_Zprev, Gh.D.Z, sizeof(double) * nz, cudaMemcpyDeviceToDevice, h->stream));
             Gh.zprev_valid = 1;
         }
         if ((rc = gen_sweep(h))) return rc;
         ++done;
+        ++Gh.age;
+        double r = NAN, sdual = NAN;
+        if (check || decide) {
+            if ((rc = gen_residuals(h, &r, &sdual))) return rc;
+        }
+        // the balancing rule of the packing engine (pk_bal_decide): a decision on
+        // iterate age a applies right after the sweep of age a + 2
+        if (Gh.bal_pending != 0 && age == Gh.bal_apply_age) {
+            cudaError_t e = gen_launch_rescale(Gh.D, Gh.bal_pending > 0 ? 2.0 : 0.5, h->stream);
+            if (e != cudaSuccess) return pdm_cuda_fail(e, "generic rescale kernel", __FILE__, __LINE__);
+            ++h->launches;
+            Gh.bal_log2 += Gh.bal_pending;
+            Gh.bal_pending = 0;
+        }
+        if (decide) {
+            Gh.bal_pending = 0;
+            if (r > Gh.bal_mu * sdual && Gh.bal_log2 < Gh.bal_lmax) Gh.bal_pending = 1;
+            else if (sdual > Gh.bal_mu * r && Gh.bal_log2 > Gh.bal_lmin) Gh.bal_pending = -1;
+            Gh.bal_apply_age = age + 2;
+        }
         if (check) {
-            if ((rc = gen_residuals(h, &rp, &rd))) return rc;
+            rp = r;
+            rd = sdual;
             if (!std::isfinite(rp + rd)) { rc = pdm_set_error(PARADMM_ENONFINITE, "residual became NaN/Inf"); break; }
             if (rp + rd <= tol) { converged = 1; break; }
         }
@@ -1565,6 +1642,31 @@ extern "C" int paradmm_gpu_get_circles(paradmm_gpu *h, int instance, double *out
     return PARADMM_OK;
 }
 
+// Device copy of n floats narrowed from host doubles (NULL in, NULL out).
+static int upload_narrowed(paradmm_gpu *h, const double *src, size_t n, float **dst)
+{
+    *dst = nullptr;
+    if (!src || n == 0) return PARADMM_OK;
+    std::vector<float> f(n);
+    for (size_t i = 0; i < n; ++i) f[i] = (float)src[i];
+    PDM_CUDA(cudaMalloc((void **)dst, sizeof(float) * n));
+    cudaError_t e = cudaMemcpyAsync(*dst, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { cudaFree(*dst); *dst = nullptr; return pdm_cuda_fail(e, "cudaMemcpyAsync", __FILE__, __LINE__); }
+    return PARADMM_OK;
+}
+
+static int pk_set_instance_circles(paradmm_gpu *h, int instance, const double *circles)
+{
+    PkHost &P = *h->pk;
+    const PkInst &I = P.inst[instance];
+    std::vector<double4> z(I.N);
+    for (int c = 0; c < I.N; ++c) z[c] = make_double4(circles[3 * c], circles[3 * c + 1], circles[3 * c + 2], 0.0);
+    PDM_CUDA(cudaMemcpyAsync(P.D.Z + I.circle_base, z.data(), sizeof(double4) * I.N, cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaStreamSynchronize(h->stream));
+    return PARADMM_OK;
+}
+
 extern "C" int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double *circles, const float *pair_duals)
 {
     ok_status();
@@ -1574,9 +1676,8 @@ extern "C" int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double
     if (instance < 0 || instance >= P.n_inst) return pdm_set_error(PARADMM_EINVAL, "instance %d out of range", instance);
     DevGuard guard(h->device);
     const PkInst &I = P.inst[instance];
-    std::vector<double4> z(I.N);
-    for (int c = 0; c < I.N; ++c) z[c] = make_double4(circles[3 * c], circles[3 * c + 1], circles[3 * c + 2], 0.0);
-    PDM_CUDA(cudaMemcpyAsync(P.D.Z + I.circle_base, z.data(), sizeof(double4) * I.N, cudaMemcpyHostToDevice, h->stream));
+    int rc = pk_set_instance_circles(h, instance, circles);
+    if (rc) return rc;
     float *d_du = nullptr;
     const size_t nd = (size_t)I.N * (I.N - 1) / 2 * 6;
     if (pair_duals) {
@@ -1584,22 +1685,63 @@ extern "C" int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double
         cudaError_t e = cudaMemcpyAsync(d_du, pair_duals, sizeof(float) * nd, cudaMemcpyHostToDevice, h->stream);
         if (e != cudaSuccess) { cudaFree(d_du); return pdm_cuda_fail(e, "cudaMemcpyAsync", __FILE__, __LINE__); }
     }
-    int rc = pk_init_instance_state(h, instance, d_du);
+    PkInitArgs A{};
+    A.pair_duals = d_du;
+    rc = pk_init_instance_state(h, instance, A);
     if (d_du) cudaFree(d_du);
     return rc;
 }
 
-extern "C" int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles, int radius_duals)
+extern "C" int paradmm_gpu_warm_start_duals(paradmm_gpu *h, int instance, const double *circles, const double *pair_duals,
+                                           const double *wall_duals, const double *radius_duals, int dual_iters)
 {
     ok_status();
     if (!h || !circles) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
     if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
     PkHost &P = *h->pk;
+    if (instance < 0 || instance >= P.n_inst) return pdm_set_error(PARADMM_EINVAL, "instance %d out of range", instance);
+    if (dual_iters < 0 || dual_iters > 100000) return pdm_set_error(PARADMM_EINVAL, "dual_iters %d out of [0, 100000]", dual_iters);
+    DevGuard guard(h->device);
+    const PkInst &I = P.inst[instance];
+    // wall factors of the instance: those of its circles, contiguous
+    const int w0 = P.circ[I.circle_base].wall_start;
+    const int w1 = P.circ[I.circle_base + I.N - 1].wall_start + P.circ[I.circle_base + I.N - 1].wall_count;
+    int rc = pk_set_instance_circles(h, instance, circles);
+    if (rc) return rc;
+    float *dp = nullptr, *dw = nullptr, *dr = nullptr;
+    if ((rc = upload_narrowed(h, pair_duals, (size_t)I.N * (I.N - 1) / 2 * 6, &dp)) ||
+        (rc = upload_narrowed(h, wall_duals, (size_t)(w1 - w0) * 3, &dw)) ||
+        (rc = upload_narrowed(h, radius_duals, (size_t)I.N, &dr))) {
+        cudaFree(dp); cudaFree(dw); cudaFree(dr);
+        return rc;
+    }
+    PkInitArgs A{};
+    A.pair_duals = dp;
+    A.wall_duals = dw;
+    A.rad_duals = dr;
+    A.dual_iters = dual_iters;
+    rc = pk_init_instance_state(h, instance, A);
+    cudaFree(dp); cudaFree(dw); cudaFree(dr);
+    return rc;
+}
+
+extern "C" int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles, int radius_duals)
+{
+    return paradmm_gpu_warm_start_all_duals(h, circles, radius_duals, 0);
+}
+
+extern "C" int paradmm_gpu_warm_start_all_duals(paradmm_gpu *h, const double *circles, int radius_duals, int dual_iters)
+{
+    ok_status();
+    if (!h || !circles) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
+    if (dual_iters < 0 || dual_iters > 100000) return pdm_set_error(PARADMM_EINVAL, "dual_iters %d out of [0, 100000]", dual_iters);
+    PkHost &P = *h->pk;
     DevGuard guard(h->device);
     std::vector<double4> z(P.n_circ);
     for (int g = 0; g < P.n_circ; ++g) z[g] = make_double4(circles[3 * g], circles[3 * g + 1], circles[3 * g + 2], 0.0);
     PDM_CUDA(cudaMemcpyAsync(P.D.Z, z.data(), sizeof(double4) * P.n_circ, cudaMemcpyHostToDevice, h->stream));
-    return pk_init_all(h, radius_duals);
+    return pk_init_all(h, radius_duals, dual_iters);
 }
 
 // ---- schedule autotuner ----
@@ -1609,7 +1751,7 @@ struct PkSnapshot {
     std::vector<void *> copy;
     std::vector<int> nmode;
     std::vector<PkStatus> status;
-    std::vector<long long> iters, upload_iter;
+    std::vector<long long> iters, upload_iter, age;
     long long it_next = 0;
 };
 
@@ -1633,6 +1775,7 @@ static int pk_snapshot_take(paradmm_gpu *h, PkSnapshot &S)
     S.status = P.status;
     S.iters = P.iters_last_call;
     S.upload_iter = P.upload_iter;
+    S.age = P.age;
     S.it_next = P.it_next;
     PDM_CUDA(cudaStreamSynchronize(h->stream));
     return PARADMM_OK;
@@ -1648,7 +1791,11 @@ static int pk_snapshot_restore(paradmm_gpu *h, const PkSnapshot &S)
     P.status = S.status;
     P.iters_last_call = S.iters;
     P.upload_iter = S.upload_iter;
+    P.age = S.age;
     P.it_next = S.it_next;
+    // the residual slots were not saved: no balancing decision may read the
+    // sums of the sweeps before the restore
+    for (int i = 0; i < P.n_inst; ++i) { P.last_swept[i] = -1; P.status[i].sd_valid = 0; }
     return PARADMM_OK;
 }
 
@@ -1760,6 +1907,52 @@ extern "C" int paradmm_gpu_create_packing_tuned(const paradmm_packing_desc *desc
     if (!best) return pdm_set_error(PARADMM_EINVAL, "no block width to try (block_width must be 0, 64 or 128)");
     if (tuning) *tuning = bt;
     *out = best;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_set_rho_balance(paradmm_gpu *h, int period, double mu, int log2_min, int log2_max)
+{
+    ok_status();
+    if (!h) return pdm_set_error(PARADMM_EINVAL, "handle is NULL");
+    if (period != 0 && period < 3) return pdm_set_error(PARADMM_EINVAL, "period %d: 0 (off) or >= 3", period);
+    if (!(mu >= 1.0) || !std::isfinite(mu)) return pdm_set_error(PARADMM_EINVAL, "mu must be finite and >= 1");
+    if (log2_min > 0 || log2_max < 0 || log2_min < -30 || log2_max > 30)
+        return pdm_set_error(PARADMM_EINVAL, "scale bounds 2^%d .. 2^%d must bracket 1, within 2^-30 .. 2^30", log2_min, log2_max);
+    if (h->pk) {
+        PkHost &P = *h->pk;
+        P.bal_period = period;
+        P.bal_mu = mu;
+        P.bal_lmin = log2_min;
+        P.bal_lmax = log2_max;
+    } else if (h->gen) {
+        GenHost &Gh = *h->gen;
+        Gh.bal_period = period;
+        Gh.bal_mu = mu;
+        Gh.bal_lmin = log2_min;
+        Gh.bal_lmax = log2_max;
+    } else {
+        return pdm_set_error(PARADMM_EINVAL, "handle has no engine");
+    }
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_rho_scale(const paradmm_gpu *h, int instance, int *log2_scale)
+{
+    ok_status();
+    if (!h || !log2_scale) return pdm_set_error(PARADMM_EINVAL, "NULL argument");
+    if (h->pk) {
+        const PkHost &P = *h->pk;
+        if (instance < 0 || instance >= P.n_inst) return pdm_set_error(PARADMM_EINVAL, "instance %d out of range", instance);
+        const PkStatus &s = P.status[instance];
+        // the scale the next sweep's radius operator uses
+        const bool after = s.bal_pass_age > 0 && P.age[instance] + 1 >= s.bal_pass_age;
+        *log2_scale = after ? s.bal_log2_new : s.bal_log2_cur;
+    } else if (h->gen) {
+        if (instance != 0) return pdm_set_error(PARADMM_EINVAL, "instance %d out of range", instance);
+        *log2_scale = h->gen->bal_log2;
+    } else {
+        return pdm_set_error(PARADMM_EINVAL, "handle has no engine");
+    }
     return PARADMM_OK;
 }
 
@@ -1917,6 +2110,8 @@ extern "C" int paradmm_gpu_shard_start(paradmm_gpu *h, int maxiter, double tol, 
     s.nonfinite = 0;
     s.nmode = P.nmode[0];
     s.mode_iter = it0;
+    s.bal_base = it0 - P.age[0];
+    s.bal_eval_from = std::max(s.bal_base + 2, P.last_swept[0] == it0 - 1 ? it0 : it0 + 2);
     PDM_CUDA(cudaMemcpyAsync(P.D.status, &s, sizeof s, cudaMemcpyHostToDevice, h->stream));
     DevCtl c{};
     c.n_active = 1;
@@ -1976,6 +2171,10 @@ extern "C" int paradmm_gpu_shard_end(paradmm_gpu *h, const void *exchange, void 
     R.dynamic = 1;
     R.tol = P.shard_tol;
     R.check_every = P.shard_check_every;
+    R.bal_period = P.bal_period;
+    R.bal_mu = P.bal_mu;
+    R.bal_lmin = P.bal_lmin;
+    R.bal_lmax = P.bal_lmax;
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = pk_launch_shard_end(P.V, P.D, R, P.shard_k, P.inst[0].nb, (const double4 *)exchange, P.d_done, s);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "shard consensus launch", __FILE__, __LINE__);
@@ -2021,6 +2220,7 @@ extern "C" int paradmm_gpu_shard_finish(paradmm_gpu *h, void *stream, paradmm_st
     P.iters_last_call[0] = std::max(0LL, last - P.shard_it0 + 1);
     P.nmode[0] = pk_pending_mode(st, last);
     P.status[0] = st;
+    if (P.iters_last_call[0] > 0) { P.age[0] += P.iters_last_call[0]; P.last_swept[0] = last; }
     P.it_next = P.shard_k;
     P.shard_running = 0;
     rc = st.nonfinite ? pdm_set_error(PARADMM_ENONFINITE, "residual became NaN/Inf") : PARADMM_OK;

@@ -32,6 +32,8 @@ struct PkGraphKey {
     int n_iter;
     double tol;
     int check_every, fallback_after, prof, cluster, n_coop, inst_grid, n_early;
+    int bal_period, bal_lmin, bal_lmax;
+    double bal_mu;
 };
 
 struct PkHost {
@@ -56,6 +58,11 @@ struct PkHost {
     PkDev D{};
     long long it_next = 0;           // global sweep counter
     std::vector<long long> upload_iter;
+    std::vector<long long> age;        // per instance: sweeps run since its state was set (balancing ages)
+    std::vector<long long> last_swept; // per instance: global index of its last sweep (grid schedule; -1: none)
+    int bal_period = 0;              // residual balancing of the penalties (paradmm_gpu_set_rho_balance)
+    double bal_mu = 10.0;
+    int bal_lmin = -1, bal_lmax = 4;
     std::vector<int> nmode;
     std::vector<PkStatus> status;    // host copy after the last launch
     std::vector<long long> iters_last_call;
@@ -107,6 +114,13 @@ struct GenHost {
     unsigned long long *d_viol = nullptr;
     int zprev_valid = 0;
     double last_primal = -1, last_dual = -1;
+    // residual balancing of the penalties (paradmm_gpu_set_rho_balance)
+    int bal_period = 0, bal_lmin = -1, bal_lmax = 4;
+    double bal_mu = 10.0;
+    long long age = 0;               // sweeps since the state was set
+    int bal_log2 = 0;                // log2 of the current penalty scale
+    int bal_pending = 0;             // +1 / -1: a doubling / halving decided, not applied yet
+    long long bal_apply_age = -1;    // age of the sweep after which it applies
 };
 
 // Run-time compiled operators (userops.cu): the X-phase kernel for operators

@@ -28,3 +28,4 @@ struct GenDev {
 cudaError_t gen_launch_phase(const GenDev &G, int phase, cudaStream_t s);
 cudaError_t gen_launch_resid(const GenDev &G, const double *Zprev, double *out, cudaStream_t s);
 cudaError_t gen_launch_violation(const GenDev &G, unsigned long long *out, cudaStream_t s);
+cudaError_t gen_launch_rescale(const GenDev &G, double t, cudaStream_t s);

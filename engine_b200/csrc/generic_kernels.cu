@@ -172,6 +172,26 @@ __global__ void gen_un(GenDev G, int do_u, int do_n)
     }
 }
 
+// A balancing step of the penalties (no reference counterpart: its hook,
+// update_outgoing_rhos, is empty, core/paradmm.c:564-566): every penalty
+// times t (t = 2 or 1/2: exact), every scaled dual U divided by t so that
+// rho U is unchanged, and N = Z - U again.
+template <typename T>
+__global__ void gen_rescale(GenDev G, double t)
+{
+    T *U = (T *)G.U, *Nn = (T *)G.N;
+    double *R = const_cast<double *>(G.RHOS);
+    const int d = G.num_dims;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < G.num_edges; e += (long long)gridDim.x * blockDim.x) {
+        R[e] *= t;
+        const long long v = G.e2v[e];
+        for (int k = 0; k < d; ++k) {
+            U[e * d + k] /= (T)t;
+            Nn[e * d + k] = (T)G.Z[d * v + k] - U[e * d + k];
+        }
+    }
+}
+
 // Sum of squares of X - Z_v(e) and of Z_v(e) - Zprev_v(e) over all (edge,
 // dim), accumulated into out[0], out[1].
 template <typename T>
@@ -268,6 +288,13 @@ cudaError_t gen_launch_resid(const GenDev &G, const double *Zprev, double *out, 
 {
     if (G.fp64) gen_resid<double><<<grid_for(G.num_edges, 256), 256, 0, s>>>(G, Zprev, out);
     else gen_resid<float><<<grid_for(G.num_edges, 256), 256, 0, s>>>(G, Zprev, out);
+    return cudaGetLastError();
+}
+
+cudaError_t gen_launch_rescale(const GenDev &G, double t, cudaStream_t s)
+{
+    if (G.fp64) gen_rescale<double><<<grid_for(G.num_edges, 256), 256, 0, s>>>(G, t);
+    else gen_rescale<float><<<grid_for(G.num_edges, 256), 256, 0, s>>>(G, t);
     return cudaGetLastError();
 }
 

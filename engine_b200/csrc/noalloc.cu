@@ -29,6 +29,8 @@
 #define NA_TILES (NA_NB * (NA_NB + 1) / 2)
 #define NA_ITEMS (NA_TILES + (NA_MAX_CIRCLES + PK_THREADS - 1) / PK_THREADS)
 #define NA_WALLS (NA_MAX_CIRCLES * NA_MAX_WALLS)
+// Tag in the state header of a buffer this entry point has initialised.
+#define NA_STATE_TAG 0x5044414e
 
 static constexpr size_t na_al(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -259,15 +261,28 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     // consensus: caller's [cx, cy, r] rows -> the kernel's (cx, cy, r, -) rows
     PDM_CUDA(cudaMemcpy2DAsync(D.Z, sizeof(double4), d_circles, 3 * sizeof(double), 3 * sizeof(double), N,
                                cudaMemcpyDeviceToDevice, s));
-    static int s_mode;
+    // State header (16 bytes after the FP32 circles): {mode, tag, 0, 0}.  The
+    // tag marks a buffer this entry point initialised; a zero-filled or
+    // foreign buffer has none and is refused when init_state = 0.  Any error
+    // after the state may have changed clears the tag, so a later call must
+    // start again with init_state = 1 rather than resume from a state whose
+    // circles and mode no longer agree.
+    static int s_hdr[4];
+    auto invalidate = [&]() {
+        static int zero[4] = {0, 0, 0, 0};
+        cudaGetLastError();
+        if (cudaMemcpyAsync(d_mode, zero, sizeof zero, cudaMemcpyHostToDevice, s) == cudaSuccess) cudaStreamSynchronize(s);
+    };
+    int s_mode;
     if (init_state) {
-        cudaError_t e = pk_launch_init(NA_V, D, 0, nullptr, g_na_grid[device], s);
-        if (e != cudaSuccess) return pdm_cuda_fail(e, "noalloc init", __FILE__, __LINE__);
+        cudaError_t e = pk_launch_init(NA_V, D, 0, PkInitArgs{}, g_na_grid[device], s);
+        if (e != cudaSuccess) { invalidate(); return pdm_cuda_fail(e, "noalloc init", __FILE__, __LINE__); }
         s_mode = PK_MODE_Z;
     } else {
-        PDM_CUDA(cudaMemcpyAsync(&s_mode, d_mode, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PDM_CUDA(cudaMemcpyAsync(s_hdr, d_mode, sizeof s_hdr, cudaMemcpyDeviceToHost, s));
         PDM_CUDA(cudaStreamSynchronize(s));
-        if (s_mode < PK_MODE_RECOMPUTE || s_mode > PK_MODE_XN)
+        s_mode = s_hdr[0];
+        if (s_hdr[1] != NA_STATE_TAG || s_mode < PK_MODE_RECOMPUTE || s_mode > PK_MODE_XN)
             return pdm_set_error(PARADMM_EINVAL, "noalloc: the state buffer was never initialised (call with init_state = 1)");
     }
 
@@ -287,8 +302,8 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         s_status.mode_iter = it0;
         memset(&s_ctl, 0, sizeof s_ctl);
         s_ctl.n_active = 1;
-        PDM_CUDA(cudaMemcpyAsync(D.status, &s_status, sizeof s_status, cudaMemcpyHostToDevice, s));
-        PDM_CUDA(cudaMemcpyAsync(D.ctl, &s_ctl, sizeof s_ctl, cudaMemcpyHostToDevice, s));
+        cudaError_t e = cudaMemcpyAsync(D.status, &s_status, sizeof s_status, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(D.ctl, &s_ctl, sizeof s_ctl, cudaMemcpyHostToDevice, s);
         PkRun R{};
         R.it0 = it0;
         R.n_iter = chunk;
@@ -296,13 +311,15 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         R.tol = tol;
         R.check_every = 1;
         R.prof = 0;
-        cudaError_t e = pk_launch_persistent(NA_V, true, D, R, g_na_grid[device], s);
-        if (e != cudaSuccess) return pdm_cuda_fail(e, "noalloc persistent launch", __FILE__, __LINE__);
-        PDM_CUDA(cudaMemcpyAsync(&s_ctl, D.ctl, sizeof s_ctl, cudaMemcpyDeviceToHost, s));
-        PDM_CUDA(cudaMemcpyAsync(&s_status, D.status, sizeof s_status, cudaMemcpyDeviceToHost, s));
-        PDM_CUDA(cudaStreamSynchronize(s));
-        if (s_ctl.err != DEV_OK)
+        if (e == cudaSuccess) e = pk_launch_persistent(NA_V, true, D, R, g_na_grid[device], s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&s_ctl, D.ctl, sizeof s_ctl, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&s_status, D.status, sizeof s_status, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { invalidate(); return pdm_cuda_fail(e, "noalloc persistent launch", __FILE__, __LINE__); }
+        if (s_ctl.err != DEV_OK) {
+            invalidate();
             return pdm_set_error(PARADMM_ETIMEOUT, "noalloc: a device-side wait ran out (%s)", pdm_dev_err_name(s_ctl.err));
+        }
         const long long last = std::min<long long>(s_status.last_iter, it0 + s_ctl.pad[0] - 1);
         const long long ran = last - it0 + 1;
         done += ran;
@@ -314,11 +331,17 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
         if (s_status.nonfinite) { status_rc = pdm_set_error(PARADMM_ENONFINITE, "noalloc: residual became NaN/Inf"); break; }
         if (s_status.converged || (long long)s_ctl.pad[0] < chunk) break;
     }
-    // consensus back to the caller's rows; the mode into the state header
-    PDM_CUDA(cudaMemcpy2DAsync(d_circles, 3 * sizeof(double), D.Z, sizeof(double4), 3 * sizeof(double), N,
-                               cudaMemcpyDeviceToDevice, s));
-    PDM_CUDA(cudaMemcpyAsync(d_mode, &s_mode, sizeof(int), cudaMemcpyHostToDevice, s));
-    PDM_CUDA(cudaStreamSynchronize(s));
+    // consensus back to the caller's rows; the mode and the tag into the
+    // state header (a NaN/Inf stop leaves a consistent state: the circles and
+    // the mode of the sweeps that ran)
+    s_hdr[0] = s_mode;
+    s_hdr[1] = NA_STATE_TAG;
+    s_hdr[2] = s_hdr[3] = 0;
+    cudaError_t e = cudaMemcpy2DAsync(d_circles, 3 * sizeof(double), D.Z, sizeof(double4), 3 * sizeof(double), N,
+                                      cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_mode, s_hdr, sizeof s_hdr, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { invalidate(); return pdm_cuda_fail(e, "noalloc write-back", __FILE__, __LINE__); }
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (stats) {
         stats->iterations = done;

@@ -111,6 +111,15 @@ struct PkStatus {
     int pad;                // 1 once the instance fell back to its plain start (per-instance schedule)
     long long mode_iter;    // sweep index the mode applies to
     unsigned long long t_begin_ns, t_end_ns;  // per-instance schedule: device clock at start / stop
+    // residual balancing of the penalties (PkRun::bal_period > 0; pk_bal_at)
+    long long bal_base;      // sweep index whose iterate is the first since the state was set (age 1)
+    long long bal_pass_age;  // age of the first iterate computed with scale 2^bal_log2_new (0: none yet)
+    long long bal_eval_from; // grid schedule: first finalisation whose residual sums may feed a decision
+    int bal_log2_cur;        // log2 of the penalty scale of the iterates before bal_pass_age
+    int bal_log2_new;        // ... from bal_pass_age on
+    double sd_last;          // per-instance schedule: dual-residual sum of the last consensus run
+    int sd_valid;            // sd_last belongs to the state the next call continues
+    int pad3;
 };
 
 // Device pointers of a packing handle (passed by value to kernels).
@@ -154,7 +163,74 @@ struct PkRun {
     int check_every;  // sweeps between stopping checks
     int prof;         // accumulate per-phase block times into DevCtl::prof
     int fallback_after;  // per-instance schedule: restart an unconverged instance from Z0 after this many sweeps (0: never)
-    int pad2;
+    int bal_period;   // residual balancing: decide every bal_period iterates (0: off; >= 3)
+    double bal_mu;    // ... double the penalties when r > mu s, halve them when s > mu r
+    int bal_lmin, bal_lmax;  // ... within scales 2^bal_lmin .. 2^bal_lmax
+};
+
+// Residual balancing of the penalties (no reference counterpart: the
+// reference's hook for it, update_outgoing_rhos, is empty,
+// core/paradmm.c:564-566).  Every penalty of an instance is scaled by 2^l.
+// Power-of-two scaling is exact, and the pair and wall operators and the
+// consensus weights are homogeneous in the penalties, so only the radius
+// operator (absolute penalty) and the scaled duals U = y / rho see it.  A
+// decision taken on the residuals of the iterate of age a (a a multiple of
+// the period) applies in the pass that produces the iterate of age a + 3:
+// that pass divides U^(a+2) by t = 2^(l_new - l_cur) right after updating
+// it (before N = Z - U), and its radius operator and every later one use
+// 2^l_new.  Ages count iterates since the state was set (create, upload,
+// warm start, fallback restart).
+struct PkBal {
+    float uf;  // factor on U right after its update in this pass (1, 1/2 or 2)
+    float rs;  // penalty scale of this pass's radius operator
+};
+
+PDM_D PkBal pk_bal_at(const PkStatus *st, long long k)
+{
+    const long long pa = __ldcg(&st->bal_pass_age);
+    const int cur = __ldcg(&st->bal_log2_cur), nw = __ldcg(&st->bal_log2_new);
+    const long long age = k - __ldcg(&st->bal_base) + 1;
+    PkBal b;
+    b.rs = ldexpf(1.0f, (pa > 0 && age >= pa) ? nw : cur);
+    b.uf = (pa > 0 && age == pa && nw != cur) ? (nw > cur ? 0.5f : 2.0f) : 1.0f;
+    return b;
+}
+
+// The balancing decision on the residuals (rp, rd) of iterate j (one thread).
+PDM_D void pk_bal_decide(PkStatus *st, const PkRun &R, long long j, double rp, double rd)
+{
+    if (R.bal_period <= 0) return;
+    const long long age = j - st->bal_base + 1;
+    if (age < R.bal_period || age % R.bal_period != 0) return;
+    const int cur = st->bal_log2_new;  // the previous decision applied at least period - 3 iterates ago
+    int nw = cur;
+    if (rp > R.bal_mu * rd && cur < R.bal_lmax) nw = cur + 1;
+    else if (rd > R.bal_mu * rp && cur > R.bal_lmin) nw = cur - 1;
+    st->bal_log2_cur = cur;
+    st->bal_log2_new = nw;
+    st->bal_pass_age = age + 3;
+}
+
+// Balancing state of a freshly set state whose first sweep is k.
+PDM_HD void pk_bal_reset(PkStatus &s, long long k)
+{
+    s.bal_base = k;
+    s.bal_pass_age = 0;
+    s.bal_eval_from = k + 2;
+    s.bal_log2_cur = s.bal_log2_new = 0;
+    s.sd_last = 0.0;
+    s.sd_valid = 0;
+}
+
+// Initial-state arguments of pk_init_state (device arrays of one instance;
+// NULL = none).
+struct PkInitArgs {
+    const float *pair_duals = nullptr;  // [pair, row-major i < j][6]
+    const float *wall_duals = nullptr;  // [wall factor of the instance][3]
+    const float *rad_duals = nullptr;   // [circle]
+    int radius_duals = 0;     // rad_duals NULL: 1 = radius duals at the radius prox's fixed point, 0 = 0
+    int dual_iters = 0;       // rounds of the reference's optimal-initialisation map after that
+    int row_lo = 0, row_hi = -1;  // stored block rows (row_hi < 0: all)
 };
 
 PDM_HD long long pk_tri(int I, int J, int nb) { return (long long)I * nb - (long long)I * (I - 1) / 2 + (J - I); }

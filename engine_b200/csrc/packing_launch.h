@@ -11,15 +11,14 @@ cudaError_t pk_launch_instances(int V, bool stream_hint, const PkDev &D, const P
                                 int n_early, unsigned *queue, int grid, int cluster, cudaStream_t s);
 cudaError_t pk_instances_max_clusters(int V, bool stream_hint, int cluster, int *clusters);
 cudaError_t pk_instances_blocks_per_sm(int V, bool stream_hint, int *blocks);
-cudaError_t pk_launch_init(int V, const PkDev &D, int inst, const float *pair_duals, int grid, cudaStream_t s,
-                           int radius_duals = 0, int row_lo = 0, int row_hi = -1);
+cudaError_t pk_launch_init(int V, const PkDev &D, int inst, const PkInitArgs &A, int grid, cudaStream_t s);
 cudaError_t pk_launch_scatter(int V, const PkDev &D, int inst, const int2 *pmap, long long npairs, const int *wmap,
                               int wall0, int nwall, const int *rmap, int rad0, int nrad, const int2 *cmap,
                               const double *Nd, const double *Ud, const double *Zd, int *flag, int grid, cudaStream_t s);
 cudaError_t pk_launch_gather(int V, const PkDev &D, int inst, const int2 *pmap, long long npairs, const int *wmap,
                              int wall0, int nwall, const int *rmap, int rad0, int nrad, const int2 *cmap,
-                             const int *wcirc, const int *rcirc, int nmode, double *Xo, double *Mo, double *No,
-                             double *Uo, double *Zo, int grid, cudaStream_t s);
+                             const int *wcirc, const int *rcirc, int nmode, float uf, double *Xo, double *Mo,
+                             double *No, double *Uo, double *Zo, int grid, cudaStream_t s);
 cudaError_t pk_launch_violation(const PkDev &D, unsigned long long *out, int grid, cudaStream_t s);
 cudaError_t pk_shard_prepare(int V, bool stream_hint, int *blocks_per_sm);
 cudaError_t pk_launch_shard_begin(int V, bool stream_hint, const PkDev &D, const PkRun &R, int grid, int nb,

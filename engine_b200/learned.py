@@ -50,6 +50,7 @@ def _bind():
         "paradmm_setmlp_features": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
         "paradmm_setmlp_predict": (C.c_int, [C.c_void_p, _P, _P]),
         "paradmm_gpu_warm_start_all": (C.c_int, [C.c_void_p, _P, C.c_int]),
+        "paradmm_gpu_warm_start_all_duals": (C.c_int, [C.c_void_p, _P, C.c_int, C.c_int]),
     }
     for k, (r, a) in sig.items():
         f = getattr(lib, k)
@@ -138,15 +139,22 @@ class Batch:
     def set_fallback(self, after_sweeps: int) -> None:
         check(self.lib.paradmm_gpu_set_fallback(self.h, int(after_sweeps)))
 
+    def set_rho_balance(self, period: int, mu: float = 10.0, log2_min: int = -1, log2_max: int = 4) -> None:
+        check(self.lib.paradmm_gpu_set_rho_balance(self.h, int(period), float(mu), int(log2_min), int(log2_max)))
+
     def fallbacks(self) -> np.ndarray:
         out = np.zeros(len(self.instances), dtype=np.int32)
         check(self.lib.paradmm_gpu_instance_fallbacks(self.h, out.ctypes.data_as(C.POINTER(C.c_int))))
         return out
 
-    def warm_start(self, circles: np.ndarray, radius_duals: int = 1) -> None:
+    def warm_start(self, circles: np.ndarray, radius_duals: int = 1, dual_iters: int = 0) -> None:
+        """Every instance from `circles`: X = Z, radius duals at the radius
+        prox's fixed point (radius_duals = 1) or 0, pair and wall duals 0,
+        then dual_iters rounds of the reference's optimal-initialisation map
+        on every factor."""
         lib = _bind()
         c = np.ascontiguousarray(circles, dtype=np.float64)
-        check(lib.paradmm_gpu_warm_start_all(self.h, c.ctypes.data_as(_P), radius_duals))
+        check(lib.paradmm_gpu_warm_start_all_duals(self.h, c.ctypes.data_as(_P), radius_duals, int(dual_iters)))
 
     def close(self):
         if self.h:
@@ -268,7 +276,8 @@ def solve_plain(instances, maxiter=20000, tol=1e-5, device=0, **batch_kw):
     return dict(wall_s=wall, device_ms=s["device_ms"], stats=st, circles=circ)
 
 
-def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, radius_duals=1, device=0, **batch_kw):
+def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, radius_duals=1, dual_iters=0, device=0,
+                  **batch_kw):
     """Learned path: network proposal -> warm start -> one solve.  With
     budget > 0, every instance still unconverged after `budget` sweeps
     restarts from its plain start (in the same launch) and gets the plain
@@ -278,7 +287,7 @@ def solve_learned(instances, net: SetMLP, budget=6000, maxiter=20000, tol=1e-5, 
     t = time.perf_counter()
     net.set_data(instances)
     prop = net.predict()
-    b.warm_start(prop, radius_duals)
+    b.warm_start(prop, radius_duals, dual_iters)
     b.set_fallback(max(budget, 0))
     s = b.solve((budget if budget > 0 else 0) + maxiter, tol)
     wall = time.perf_counter() - t

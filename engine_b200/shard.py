@@ -120,3 +120,42 @@ def solve(desc: dict, maxiter: int, tol: float, group=None, poll_every: int = 64
             dist.all_reduce(t, group=group)
 
     return shard, run_sharded(shard, exchange, allreduce, maxiter, tol, poll_every)
+
+
+# ------------------------------------------------------- batches over ranks
+def split_instances(sizes, world: int, rank: int) -> list[int]:
+    """Indices of the instances rank `rank` of `world` solves when a batch of
+    independent packing instances is dealt over the ranks (no communication
+    between them).  The instances are taken largest first (a sweep's work
+    grows with N^2) and dealt in snake order 0, 1, .., R-1, R-1, .., 0, 0, ..
+    so every rank gets a near-equal share of the work; each rank's list keeps
+    that order (largest first).  Every index goes to exactly one rank."""
+    order = sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i))
+    mine = []
+    for k, i in enumerate(order):
+        lap, pos = divmod(k, world)
+        owner = pos if lap % 2 == 0 else world - 1 - pos
+        if owner == rank:
+            mine.append(i)
+    return mine
+
+
+def gather_instances(mine: list[int], rows: list, total: int, world: int, group=None):
+    """Per-instance results of a batch dealt by split_instances, back in the
+    batch's order on every rank: rows[k] belongs to instance mine[k].  With
+    world > 1 every rank takes part (torch.distributed all_gather_object)."""
+    parts = [(list(mine), list(rows))]
+    if world > 1:
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, (list(mine), list(rows)), group=group)
+    out = [None] * total
+    for idx, rs in parts:
+        for i, r in zip(idx, rs):
+            if out[i] is not None:
+                raise ValueError(f"instance {i} reported by two ranks")
+            out[i] = r
+    missing = [i for i, r in enumerate(out) if r is None]
+    if missing:
+        raise ValueError(f"{len(missing)} instances reported by no rank (first {missing[0]})")
+    return out

@@ -199,6 +199,54 @@ int paradmm_gpu_get_circles(paradmm_gpu *h, int instance, double *out);
  * [u_cx_i, u_cy_i, u_r_i, u_cx_j, u_cy_j, u_r_j]. */
 int paradmm_gpu_warm_start(paradmm_gpu *h, int instance, const double *circles, const float *pair_duals);
 
+/* The reference's warm-start contract, initialize_X_N_Z_M_U_optimal(G,
+ * Zinit, Uinit, maxiter) (core/paradmm.c:266-375), for one instance, on the
+ * device: Z from `circles`, X_e = Z_v(e) on every edge, the duals U from
+ * Uinit, then `dual_iters` rounds of the reference's per-factor map
+ *     X~ = prox_f(Z - U),  U <- X~ - (Z - U)
+ * (its loop at core/paradmm.c:349-357), each factor on its own with its own
+ * penalties, so that a dual reaching the map's fixed point makes Z a fixed
+ * point of that factor's prox.  N = Z - U and M = X + U follow.  Uinit:
+ *   pair_duals    6 per pair i < j, row-major: [u_cx_i, u_cy_i, u_r_i,
+ *                 u_cx_j, u_cy_j, u_r_j];
+ *   wall_duals    3 per wall factor [u_cx, u_cy, u_r], circle by circle,
+ *                 each circle's walls in the order they were given;
+ *   radius_duals  1 per circle;
+ * any of them NULL = 0.  dual_iters = 0 takes Uinit as it is (unlike the
+ * reference, whose U is left unset then, core/paradmm.c:278).  The state is
+ * kept in FP32.  Resets the instance's penalty scale to 1. */
+int paradmm_gpu_warm_start_duals(paradmm_gpu *h, int instance, const double *circles, const double *pair_duals,
+                                 const double *wall_duals, const double *radius_duals, int dual_iters);
+
+/* Residual balancing of the penalties (adaptive rho).  The reference has a
+ * hook for it and nothing in it: update_outgoing_rhos (core/paradmm.c:564-566,
+ * called at the end of updateZ, :671 and :893) is empty; the drop-in
+ * update_outgoing_rhos of this library stays empty too, and the paradmm.h
+ * sweep functions never balance.  On a handle, after this call, every
+ * `period` iterates (counted from the state the handle was created, uploaded
+ * or warm-started with; ages a = period, 2 period, ...) the residuals r, s of
+ * that iterate decide: r > mu s doubles every penalty of the instance (as long
+ * as its scale stays <= 2^log2_max), s > mu r halves them (scale >=
+ * 2^log2_min), else nothing.  A decision on the iterate of age a applies
+ * right after the sweep of age a + 2: RHOS times t (t = 2 or 1/2) and the
+ * scaled duals U divided by t (N = Z - U follows), so rho U is unchanged.
+ * Power-of-two scaling is exact, and the pair and wall operators and the
+ * consensus weights are homogeneous in the penalties, so only the radius
+ * operator and the duals feel it: the FP64 generic engine reproduces the
+ * same rule applied to the reference's own updateG bit for bit.  period = 0
+ * switches it off (the default); otherwise period >= 3 and mu >= 1.  A new
+ * state (upload, warm start, fallback restart) returns the scale to 1.
+ * Downloads give U in the current scale; RHOS of the host graph is not
+ * written (the current penalties are RHOS x 2^scale, paradmm_gpu_rho_scale).
+ * In the grid schedule, an instance resumed by a later call after it had
+ * stopped skips the decisions that fall on its first two sweeps of that
+ * call.  With exponent-2 radius rewards keep rho_radius 2^log2_min > 2: the
+ * radius operator is convex only there (packing/host.c:10-29). */
+int paradmm_gpu_set_rho_balance(paradmm_gpu *h, int period, double mu, int log2_min, int log2_max);
+
+/* log2 of the penalty scale instance `instance` will use in its next sweep. */
+int paradmm_gpu_rho_scale(const paradmm_gpu *h, int instance, int *log2_scale);
+
 /* In-call fallback for warm starts (per-instance schedule only; no reference
  * counterpart).  With after_sweeps > 0, every later paradmm_gpu_solve call
  * restarts an instance that has not converged after after_sweeps sweeps of
@@ -341,8 +389,12 @@ int paradmm_gpu_shard_finish(paradmm_gpu *h, void *stream, paradmm_stats *stats)
  *              16-byte aligned: the FP32 edge state in the engine's layout
  *              (opaque to the caller).  With init_state = 1 it is first set to the plain
  *              start X_e = Z_v(e), U = 0; with init_state = 0 it must hold
- *              the state a previous call left, so consecutive calls continue
- *              one solve.
+ *              the state a previous successful (or NaN/Inf-stopped) call
+ *              left, so consecutive calls continue one solve.  A buffer this
+ *              entry point never initialised (zero-filled, say) is refused
+ *              with PARADMM_EINVAL, and so is one whose last call ended in
+ *              any other error: the state then has to start again with
+ *              init_state = 1.
  * All scratch (tables, consensus partial sums, residual slots, barrier
  * control) lives in one fixed array of PARADMM_NOALLOC_SCRATCH_BYTES inside
  * this library, present on every GPU that loads it until the process exits.

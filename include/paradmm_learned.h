@@ -66,6 +66,12 @@ int paradmm_setmlp_predict(paradmm_setmlp *net, const double *init, double *out)
  * (a r^(a-1) / rho for exponent a), else 0. */
 int paradmm_gpu_warm_start_all(paradmm_gpu *h, const double *circles, int radius_duals);
 
+/* The same, then `dual_iters` rounds of the reference's optimal-initialisation
+ * map on every factor's duals (paradmm_gpu_warm_start_duals with Uinit = the
+ * duals above): X~ = prox_f(Z - U), U <- X~ - (Z - U)
+ * (core/paradmm.c:349-357).  dual_iters = 0 is paradmm_gpu_warm_start_all. */
+int paradmm_gpu_warm_start_all_duals(paradmm_gpu *h, const double *circles, int radius_duals, int dual_iters);
+
 #ifdef __cplusplus
 }
 #endif

@@ -158,6 +158,73 @@ int orc_packing_run(orc_packing *P, int iters, int nthreads, double tol, double 
     return done;
 }
 
+static void orc_residuals(const graph *G, const double *Zprev, double *r, double *s)
+{
+    const int d = G->num_dims;
+    double sp = 0, sd = 0;
+    for (int e = 0; e < G->num_edges; e++) {
+        const int v = G->edgeix_to_varlistix[e];
+        for (int k = 0; k < d; k++) {
+            const double t = G->X[d * e + k] - G->Z[d * v + k];
+            const double q = G->Z[d * v + k] - Zprev[d * v + k];
+            sp += t * t;
+            sd += q * q;
+        }
+    }
+    const double n = (double)G->num_edges * d;
+    *r = sqrt(sp / n);
+    *s = sqrt(sd / n);
+}
+
+int orc_packing_run_balanced(orc_packing *P, int iters, double tol, int period, double mu, int lmin, int lmax,
+                             double *trace)
+{
+    graph *G = &P->G;
+    if (period < 3) return -1;
+    const int d = G->num_dims;
+    const size_t zn = (size_t)d * G->num_vars;
+    double *Zprev = malloc(sizeof(double) * zn);
+    int done = 0, log2s = 0, pending = 0, apply_age = -1;
+    for (int it = 0; it < iters; it++) {
+        const int age = it + 1;
+        memcpy(Zprev, G->Z, sizeof(double) * zn);
+        updateG(G);
+        done++;
+        double r, s;
+        orc_residuals(G, Zprev, &r, &s);
+        int applied = 0;
+        if (age == apply_age && pending != 0) {
+            const double t = pending > 0 ? 2.0 : 0.5;
+            for (int e = 0; e < G->num_edges; e++) G->RHOS[e] *= t;
+            for (int e = 0; e < G->num_edges; e++) {
+                const int v = G->edgeix_to_varlistix[e];
+                for (int k = 0; k < d; k++) {
+                    G->U[d * e + k] /= t;
+                    G->N[d * e + k] = G->Z[d * v + k] - G->U[d * e + k];
+                }
+            }
+            log2s += pending;
+            applied = pending;
+            pending = 0;
+        }
+        if (age % period == 0) {
+            if (r > mu * s && log2s < lmax) pending = 1;
+            else if (s > mu * r && log2s > lmin) pending = -1;
+            else pending = 0;
+            apply_age = age + 2;
+        }
+        if (trace) {
+            trace[4 * (size_t)it + 0] = r;
+            trace[4 * (size_t)it + 1] = s;
+            trace[4 * (size_t)it + 2] = log2s;
+            trace[4 * (size_t)it + 3] = applied;
+        }
+        if (tol > 0 && r + s <= tol) break;
+    }
+    free(Zprev);
+    return done;
+}
+
 static double now_s(void)
 {
     struct timespec ts;

@@ -54,6 +54,30 @@ void orc_packing_metrics(orc_packing *P, const double *Zprev, double out[4]);
  * early when tol > 0 and r + s <= tol.  Returns the sweeps done. */
 int orc_packing_run(orc_packing *P, int iters, int nthreads, double tol, double *trace);
 
+/* Residual balancing of the penalties between sweeps.  The reference has a
+ * hook for it and nothing in it: update_outgoing_rhos (core/paradmm.c:564-566,
+ * called at the end of updateZ, :671) is empty.  This is the rule the engine
+ * implements (paradmm_gpu_set_rho_balance), restated over the reference's
+ * own updateG:
+ *   - sweeps are counted from the state this call starts from (the sweep
+ *     that produces iterate a has age a = 1, 2, ...);
+ *   - after every sweep the residuals r_a, s_a are computed (out[0..1] of
+ *     orc_packing_metrics, without the O(N^2) packing metrics);
+ *   - at ages a with a % period == 0 the rule decides from (r_a, s_a):
+ *     r_a > mu s_a and log2 scale < lmax: double every penalty;
+ *     s_a > mu r_a and log2 scale > lmin: halve every penalty; else nothing;
+ *   - a decision made at age a is applied after the sweep of age a + 2:
+ *     every RHOS entry times t (t = 2 or 1/2), every U entry divided by t
+ *     (the scaled dual keeps rho U fixed), N = Z - U.
+ * Scaling by a power of two is exact, and the pair and wall operators and
+ * the consensus weights are homogeneous in the penalties, so only the radius
+ * operator (absolute rho) and the dual scale see the change.  period >= 3.
+ * trace (iters x 4, may be NULL): r, s, log2 scale in force for the next
+ * sweep, and +1 / -1 / 0 for a doubling / halving / nothing applied after
+ * that sweep.  Returns the sweeps done (stops when tol > 0 and r + s <= tol). */
+int orc_packing_run_balanced(orc_packing *P, int iters, double tol, int period, double mu, int lmin, int lmax,
+                             double *trace);
+
 /* Wall-clock seconds of `iters` sweeps: updateG (nthreads == 0) or one
  * updateGOpenMP(G, iters, nthreads) call. */
 double orc_time_sweeps(graph *G, int iters, int nthreads);

@@ -6,7 +6,7 @@
  * A plain-C restatement of the reference parADMM CPU path, written from the
  * reference's behaviour:
  *   graph construction  core/paradmm.c:79-120, 381-466
- *   initialisation      core/paradmm.c:188-226
+ *   initialisation      core/paradmm.c:188-226, 266-375 (optimal)
  *   sweep               core/paradmm.c:569-741  (updateXM, updateZ, updateUN)
  *   OpenMP sweep        core/paradmm.c:949-1092 (same arithmetic, threads)
  *   packing operators   packing/host.c:10-132
@@ -151,6 +151,47 @@ void initialize_X_N_Z_M_U_zeros(graph *G)
     G->M = calloc(le, sizeof(double));
     G->U = calloc(le, sizeof(double));
     G->Z = calloc(lv, sizeof(double));
+}
+
+/* core/paradmm.c:266-375: Z = Zinit, X_e = Z_v(e), then for every factor
+ * `maxiter` rounds of  X~ = op(X - U),  U = -(X - U) + X~  from U = Uinit;
+ * N = X - U, M = X + U.  Allocates the state arrays as the reference does.
+ * With maxiter = 0 the reference leaves U unset; here it is then 0. */
+void initialize_X_N_Z_M_U_optimal(graph *G, double Zinit[], double Uinit[], int maxiter)
+{
+    const int d = G->num_dims;
+    size_t le = (size_t)d * G->num_edges, lv = (size_t)d * G->num_vars;
+    G->X = malloc(sizeof(double) * le);
+    G->N = malloc(sizeof(double) * le);
+    G->M = malloc(sizeof(double) * le);
+    G->U = calloc(le, sizeof(double));
+    G->Z = malloc(sizeof(double) * lv);
+    for (size_t i = 0; i < lv; i++) G->Z[i] = Zinit[i];
+    for (int v = 0; v < G->num_vars; v++)
+        for (int q = 0; q < G->varix_to_numedges[v]; q++) {
+            const int e = G->varix_to_edgelistix[v][q];
+            for (int k = 0; k < d; k++) G->X[(size_t)e * d + k] = Zinit[(size_t)v * d + k];
+        }
+    double *xmu = malloc(sizeof(double) * le), *xi = malloc(sizeof(double) * le);
+    double *rh = malloc(sizeof(double) * (size_t)G->num_edges);
+    for (size_t i = 0; i < le; i++) { xmu[i] = G->X[i] - Uinit[i]; xi[i] = G->X[i]; }
+    for (int e = 0; e < G->num_edges; e++) rh[e] = G->RHOS[e];
+    for (int f = 0; f < G->num_opts; f++) {
+        const int ne = G->operatorix_to_numedges[f], e0 = G->operatorix_to_edgelistix[f][0];
+        const size_t o = (size_t)d * e0;
+        for (int it = 0; it < maxiter; it++) {
+            G->list_of_operators_functions_pointers[f](&xi[o], &xmu[o], &rh[e0], ne, d,
+                                                       G->list_of_operators_param_pointers[f]);
+            for (int j = 0; j < d * ne; j++) {
+                G->U[o + j] = -xmu[o + j] + xi[o + j];
+                xmu[o + j] = G->X[o + j] - G->U[o + j];
+            }
+        }
+    }
+    for (size_t i = 0; i < le; i++) { G->M[i] = G->X[i] + G->U[i]; G->N[i] = xmu[i]; }
+    free(xi);
+    free(rh);
+    free(xmu);
 }
 
 /* ---------------------------------------------------- packing operators */

@@ -26,8 +26,13 @@ _cache: dict[str, C.CDLL] = {}
 
 
 def ensure_built() -> None:
-    if not os.path.exists(PORT) or (os.path.isdir("/root/reference") and not os.path.exists(REF)):
-        subprocess.run(["make", "-C", ORACLE], check=True, capture_output=True)
+    """Builds what is missing: the restatement always, the reference's own
+    build when PARADMM_REFERENCE names the reference tree."""
+    ref_tree = os.environ.get("PARADMM_REFERENCE", "")
+    want_ref = bool(ref_tree) and os.path.isdir(ref_tree) and not os.path.exists(REF)
+    if not os.path.exists(PORT) or want_ref:
+        cmd = ["make", "-C", ORACLE] + ([f"REF={ref_tree}"] if want_ref else [])
+        subprocess.run(cmd, check=True, capture_output=True)
 
 
 def _load(path: str) -> C.CDLL:
@@ -57,6 +62,12 @@ def _load(path: str) -> C.CDLL:
     L.startG.argtypes = [C.POINTER(Graph), C.c_int]
     L.addNode.argtypes = [C.POINTER(Graph), C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     L.initialize_RHOS_APHAS.argtypes = [C.POINTER(Graph), C.c_double, C.c_double]
+    L.initialize_X_N_Z_M_U_optimal.argtypes = [C.POINTER(Graph), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                 C.c_int]
+    L.initialize_X_N_Z_M_U_optimal.restype = None
+    L.orc_packing_run_balanced.restype = C.c_int
+    L.orc_packing_run_balanced.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int,
+                                           C.c_void_p]
     L.max_alpha_radius.restype = C.c_double
     L.max_alpha_radius.argtypes = [C.c_double, C.c_double, C.c_double]
     for n in ("disk_collision_variable_radius", "disk_plane_collision_variable_radius",
@@ -118,6 +129,51 @@ class OraclePacking:
 
     def state(self) -> dict:
         return self.G.state()
+
+    def run_balanced(self, iters: int, period: int, mu: float, lmin: int, lmax: int, tol: float = 0.0):
+        """orc_packing_run_balanced: updateG with residual balancing of the
+        penalties between sweeps; trace rows (r, s, log2 scale, applied)."""
+        tr = np.zeros((iters, 4))
+        n = self.lib.orc_packing_run_balanced(self.P, iters, tol, period, mu, lmin, lmax, tr.ctypes.data)
+        assert n >= 0, "orc_packing_run_balanced refused its arguments"
+        return n, tr[:n]
+
+    def duals(self, order: int = 0):
+        """The duals U of the current state in the engine's warm-start order
+        (paradmm_gpu_warm_start_duals): pair_duals [P, 6] (pairs i < j
+        row-major: u_cx_i, u_cy_i, u_r_i, u_cx_j, u_cy_j, u_r_j),
+        wall_duals [N * nwalls, 3] (circle by circle, walls in order) and
+        radius_duals [N]; radius edges give their dim 0.  Graph order 0
+        (packing/host.c: radius factors, then walls, then pairs)."""
+        assert order == 0
+        N, nw = self.N, len(self.walls)
+        U = self.G.arr("U").reshape(-1, 2)
+        rad = U[:N, 0].copy()
+        wall = np.zeros((N * nw, 3))
+        for w in range(nw):
+            e = N + 2 * (w * N + np.arange(N))
+            wall[np.arange(N) * nw + w, 0:2] = U[e]
+            wall[np.arange(N) * nw + w, 2] = U[e + 1, 0]
+        base = N + 2 * nw * N
+        q = U[base:].reshape(-1, 4, 2)
+        pair = np.stack([q[:, 0, 0], q[:, 0, 1], q[:, 1, 0], q[:, 2, 0], q[:, 2, 1], q[:, 3, 0]], axis=1)
+        return pair, wall, rad
+
+    def circles(self) -> np.ndarray:
+        Z = self.G.arr("Z").reshape(-1, 4)
+        return np.ascontiguousarray(Z[:, :3])
+
+    def set_circles_plain(self, circles: np.ndarray) -> None:
+        """Plain start from given circles: Z, X = N = M = Z_v(e), U = 0."""
+        G = self.G
+        Z = G.arr("Z").reshape(-1, 4)
+        Z[:, 0:3] = circles
+        Z[:, 3] = circles[:, 2]
+        Zv = Z.reshape(-1, 2)
+        v = np.ctypeslib.as_array(G.edgeix_to_varlistix, shape=(G.num_edges,))
+        for k in ("X", "N", "M"):
+            G.arr(k).reshape(-1, 2)[:] = Zv[v]
+        G.arr("U")[:] = 0.0
 
     def set_state(self, st: dict) -> None:
         G = self.G

@@ -105,3 +105,61 @@ def test_harness_metrics_match_numpy():
         for j in range(i + 1, N):
             viol = max(viol, rad[i] + rad[j] - float(np.hypot(*(c[i] - c[j]))))
     assert abs(viol - m[2]) <= 1e-12 and abs(rad.sum() - m[3]) <= 1e-12
+
+
+def test_balanced_run_restates_the_rule():
+    """orc_packing_run_balanced (the residual-balancing rule the engine
+    implements, over the reference's own updateG): before the first decision
+    applies it is the plain run bit for bit; afterwards every penalty is its
+    base value times 2^(log2 scale), the scaled duals moved by the inverse
+    factor (so rho U is continuous), and N = Z - U."""
+    lib = oracle_lib.best()
+    N = 24
+    walls = eb.box_walls(1.0, 1.0)
+    a = oracle_lib.OraclePacking(lib, N, walls, 2.0)
+    b = oracle_lib.OraclePacking(lib, N, walls, 2.0)
+    a.init(11, 1.0, 1.0, 0.05, 10.0, 5.0, 1.0)
+    b.init(11, 1.0, 1.0, 0.05, 10.0, 5.0, 1.0)
+    base = a.G.arr("RHOS").copy()
+    n, tr = a.run_balanced(26, 25, 2.0, -1, 4)  # the first decision (age 25) applies after sweep 27
+    b.run(26, trace=False)
+    _same(a.state(), b.state())
+    assert not tr[:, 3].any()
+    # one more sweep each: the balanced run now applies its first decision
+    n2, tr2 = a.run_balanced(200, 25, 2.0, -1, 4)
+    assert n2 == 200 and tr2[:, 3].any()
+    G = a.G
+    l2 = int(tr2[-1, 2])
+    assert np.array_equal(G.arr("RHOS"), base * 2.0 ** l2)
+    U, Z = G.arr("U"), G.arr("Z")
+    v = np.ctypeslib.as_array(G.edgeix_to_varlistix, shape=(G.num_edges,))
+    applied_last = np.nonzero(tr2[:, 3])[0][-1]
+    if applied_last == len(tr2) - 1:  # N was reset from the rescaled U right after the last sweep
+        assert np.array_equal(G.arr("N"), Z[v] - U)
+    # a period below 3 is refused
+    assert a.lib.orc_packing_run_balanced(a.P, 5, 0.0, 2, 10.0, -1, 4, None) == -1
+
+
+@pytest.mark.parametrize("maxiter", [1, 7])
+def test_port_optimal_init_bit_identical_to_reference(maxiter):
+    """initialize_X_N_Z_M_U_optimal (core/paradmm.c:266-375) restated in the
+    port: same arrays as the reference's own, bit for bit, from a mid-solve
+    Zinit and Uinit; the engine's device-side dual initialiser is checked
+    against it on the GPU."""
+    import ctypes as C
+    ref = oracle_lib.ref()
+    if ref is None:
+        pytest.skip("reference sources not available here")
+    port = oracle_lib.port()
+    N = 30
+    walls = eb.box_walls(1.0, 1.0)
+    out = []
+    for lib in (ref, port):
+        o = oracle_lib.OraclePacking(lib, N, walls, 2.0)
+        o.init(5, 1.0, 1.0, 0.05, 10.0, 5.0, 1.0)
+        o.run(120, trace=False)
+        z, u = o.G.arr("Z").copy(), o.G.arr("U").copy()
+        lib.initialize_X_N_Z_M_U_optimal(o.graph_ptr(), z.ctypes.data_as(C.POINTER(C.c_double)),
+                                         u.ctypes.data_as(C.POINTER(C.c_double)), maxiter)
+        out.append(o.state())
+    _same(out[0], out[1])
