@@ -17,11 +17,13 @@ Arms:
                     paradmm.h call updateGOpenMP(G, sweeps, threads) on a host
                     graph, with its uploads and downloads in the timed region.
                     `cpu_baseline` is the reference's updateGOpenMP on the
-                    same N = 8000 graph, 10 sweeps, all host cores.
+                    same N = 8000 graph, 10 sweeps, as many host threads as
+                    its int loop bounds allow there (8).
   --impl reference  the reference's own CPU path (updateGOpenMP of
                     core/paradmm.c, compiled from its sources into oracle/_ref
-                    with its -Ofast flags) on all host cores, on the same
-                    N = 8000 graph: W warm-up sweeps, then K timed sweeps
+                    with its -Ofast flags) on up to all host cores (8 on
+                    this graph: past that its int loop bounds overflow), on
+                    the same N = 8000 graph: W warm-up sweeps, then K timed sweeps
                     (fewer only when K sweeps would exceed REF_BUDGET_S; the
                     line says how many ran).
 
@@ -236,6 +238,9 @@ def reference_run(n: int, warmup: int, sweeps: int, threads: int, budget_s: floa
     P = oracle_lib.OraclePacking(lib, n, eb.box_walls(BOX_W, BOX_H), EXPONENT)
     P.init(SEED, BOX_W, BOX_H, RMAX, RHO, RHO_R, ALPHA)
     build_s = time.time() - t
+    # the reference's updateGOpenMP overflows its int loop bounds past this
+    # many threads on this graph (oracle_lib.omp_threads)
+    threads = oracle_lib.omp_threads(P.G, threads)
     run = sweeps
     if warmup:
         wt = lib.orc_time_sweeps(P.graph_ptr(), warmup, threads)
@@ -244,18 +249,20 @@ def reference_run(n: int, warmup: int, sweeps: int, threads: int, budget_s: floa
     dt = lib.orc_time_sweeps(P.graph_ptr(), run, threads)
     E = P.G.num_edges
     P.close()
-    return {"rate": E * run / dt, "seconds": dt, "edges": E, "kind": kind, "sweeps": run, "build_s": build_s}
+    return {"rate": E * run / dt, "seconds": dt, "edges": E, "kind": kind, "sweeps": run, "build_s": build_s,
+            "threads": threads}
 
 
 def run_reference_arm(args):
     world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
     n = args.circles
-    r = reference_run(n, args.warmup, args.steps, threads, REF_BUDGET_S)
+    r = reference_run(n, args.warmup, args.steps, os.cpu_count() or 1, REF_BUDGET_S)
+    threads = r["threads"]
     sample = (f"the full N={n} graph ({r['edges']} edges), {args.warmup} warm-up + {r['sweeps']} timed sweeps of "
-              f"updateGOpenMP in one call, {threads} threads (nproc {os.cpu_count()})")
+              f"updateGOpenMP in one call, {threads} threads (nproc {os.cpu_count()}; the reference's int loop "
+              f"bounds, id * N / numthreads at core/paradmm.c:990, overflow past {threads} on this graph)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": r["rate"], "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / r["sweeps"] * 1e3,
@@ -469,11 +476,12 @@ def run_engine_arm(args):
             ttr = {"error": str(ex)[:200]}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        r = reference_run(n, 1, CPU_SWEEPS, threads)
-        cpu = {"value": r["rate"], "unit": METRIC, "cores": threads, "kind": r["kind"],
+        r = reference_run(n, 1, CPU_SWEEPS, os.cpu_count() or 1)
+        cpu = {"value": r["rate"], "unit": METRIC, "cores": r["threads"], "kind": r["kind"],
                "sample": f"the same N={n} graph ({r['edges']} edges), 1 warm-up + {r['sweeps']} timed sweeps of "
-                         f"the reference updateGOpenMP ({r['seconds']:.1f} s), nproc {os.cpu_count()}"}
+                         f"the reference updateGOpenMP ({r['seconds']:.1f} s), {r['threads']} threads (nproc "
+                         f"{os.cpu_count()}; the reference's int loop bounds, id * N / numthreads at "
+                         f"core/paradmm.c:990, overflow past {r['threads']} on this graph)"}
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,

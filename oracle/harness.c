@@ -137,9 +137,25 @@ void orc_packing_metrics(orc_packing *P, const double *Zprev, double out[4])
     out[3] = total;
 }
 
+/* The reference's updateGOpenMP splits its loops as id * N / numthreads in
+ * int (core/paradmm.c:964-965, 990-991, ...), N up to num_edges * num_dims:
+ * more threads than INT_MAX / N overflow and write outside the arrays, so
+ * the harness never asks for more. */
+static int orc_safe_threads(const graph *G, int nthreads)
+{
+    long long n = (long long)G->num_edges * G->num_dims;
+    if (G->num_opts > n) n = G->num_opts;
+    if (G->num_vars > n) n = G->num_vars;
+    if (n < 1) n = 1;
+    const long long cap = 2147483647LL / n;
+    if (nthreads > cap) nthreads = (int)(cap < 1 ? 1 : cap);
+    return nthreads;
+}
+
 int orc_packing_run(orc_packing *P, int iters, int nthreads, double tol, double *trace)
 {
     graph *G = &P->G;
+    if (nthreads > 0) nthreads = orc_safe_threads(G, nthreads);
     const size_t zn = (size_t)G->num_dims * G->num_vars;
     double *Zprev = malloc(sizeof(double) * zn);
     int done = 0;
@@ -234,6 +250,7 @@ static double now_s(void)
 
 double orc_time_sweeps(graph *G, int iters, int nthreads)
 {
+    if (nthreads > 0) nthreads = orc_safe_threads(G, nthreads);
     const double t0 = now_s();
     if (nthreads == 0) for (int it = 0; it < iters; it++) updateG(G);
     else updateGOpenMP(G, iters, nthreads);

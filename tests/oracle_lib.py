@@ -78,6 +78,17 @@ def _load(path: str) -> C.CDLL:
     return L
 
 
+def omp_threads(G, want: int) -> int:
+    """The most host threads (<= want) the reference's updateGOpenMP can use
+    on graph G.  It splits each loop as id * N / numthreads in int
+    (core/paradmm.c:964-965, 990-991, 1002-1003, 1044-1045, 1069-1070), with
+    N up to num_edges * num_dims; past INT_MAX / N threads the product
+    overflows and the threads write outside the state arrays (the N = 8000
+    bench graph, 2 x 128,056,000 components, allows 8)."""
+    n = max(int(G.num_edges) * int(G.num_dims), int(G.num_opts), int(G.num_vars), 1)
+    return max(1, min(int(want), (2 ** 31 - 1) // n))
+
+
 def port() -> C.CDLL:
     ensure_built()
     return _load(PORT)
@@ -114,6 +125,8 @@ class OraclePacking:
         self.lib.orc_packing_init(self.P, seed, W, H, rmax, rho, rho_radius, alpha)
 
     def run(self, iters: int, nthreads: int = 0, tol: float = 0.0, trace: bool = True):
+        if nthreads > 0:
+            nthreads = omp_threads(self.G, nthreads)
         tr = np.zeros((iters, 4)) if trace else None
         n = self.lib.orc_packing_run(self.P, iters, nthreads, tol, tr.ctypes.data if trace else None)
         return n, (tr[:n] if trace else None)
