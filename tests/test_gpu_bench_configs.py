@@ -5,11 +5,13 @@ variable's consensus sum runs in one thread in insertion order,
 core/paradmm.c:949-1092).
 
   * the bench workload: N = 8000 circles in a 2 x 1 box, radii in
-    [0, 0.01], rho 10 / 5, alpha 1, exponent 2, the bench's seed -- one
-    sweep from the seeded start (overlapping pairs present), four more
-    free-running, and one sweep teacher-forced from reference iterate 50;
+    [0, 0.01], rho 10 / 5, alpha 1, exponent 2, the bench's seed --
+    teacher-forced (one engine sweep from reference iterate k against
+    iterate k + 1) at k = 0 .. 4 and 50, overlapping pairs present; and five
+    free-running sweeps from the seeded start, checked on the consensus Z;
   * configuration 1: N = 2000 in the unit box, radii in [0, 0.05] --
-    teacher-forced at iterates 0, 50 and 500, and 8 free-running sweeps;
+    teacher-forced at k = 0 .. 7, 50 and 500, and eight free-running sweeps
+    checked on Z;
   * the batched workload: instances of the 512-instance time-to-residual
     batch (N uniform in [20, 400]), each set inside the batch handle to a
     reference iterate (Z^k and U^k through paradmm_gpu_warm_start_duals) and
@@ -17,8 +19,15 @@ core/paradmm.c:949-1092).
     its next two consensus iterates are compared with the reference's.
 
 Tolerance: the packing engine's per-iterate max |difference| 1e-4 (FP32
-edge state).  The N = 8000 case holds two FP64 host graphs (about 13 GB
-each) and runs about 50 reference sweeps on all host cores.
+edge state).  Free-running, only Z is held to it: at these sizes the
+random start has pairs with nearly coincident centres, whose projection
+direction amplifies FP32 rounding of the edge state, and FP32 arithmetic on
+its own -- a numpy restatement with none of the engine's code -- leaves the
+reference's per-edge X and U by 1.2e-4 at the second sweep of
+configuration 1 while Z stays within 2e-7
+(test_fp32_horizon.py::test_fp32_per_edge_horizon_at_configuration1).  The
+N = 8000 case holds two FP64 host graphs (about 13 GB each) and runs about
+50 reference sweeps on up to 8 host threads.
 """
 import ctypes as C
 import os
@@ -74,27 +83,49 @@ def _copy_state(dst, src):
         dst.arr(k)[:] = src.arr(k)
 
 
+def _zdiff(G, H) -> float:
+    return float(np.max(np.abs(G.arr("Z") - H.arr("Z"))))
+
+
+def _teacher_forced(pg, orc, ks, N):
+    """One engine sweep from each reference iterate k in ks (ascending)
+    against reference iterate k + 1; returns the worst max |difference|."""
+    worst, done = 0.0, 0
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
+        assert h.engine() == eb.ENGINE_PACKING
+        for k in ks:
+            orc.run(k - done, THREADS, trace=False)
+            _copy_state(pg.G, orc.G)
+            h.upload(pg.G)
+            h.iterate(1)
+            h.download(pg.G)
+            orc.run(1, THREADS, trace=False)
+            done = k + 1
+            d = _maxdiff(pg.G, orc.G)
+            assert d <= TOL_F32, f"N={N}, teacher-forced from iterate {k}: max |diff| {d}"
+            worst = max(worst, d)
+    return worst
+
+
+def _free_running_z(pg, orc, sweeps, N):
+    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
+        for k in range(sweeps):
+            h.iterate(1)
+            h.download(pg.G)
+            orc.run(1, THREADS, trace=False)
+            d = _zdiff(pg.G, orc.G)
+            assert d <= TOL_F32, f"N={N}, free-running sweep {k + 1}: max |diff| of Z {d}"
+
+
 def test_bench_workload_n8000():
     import bench
     N = bench.N_CIRCLES
     pg, orc, circles = _pair(N, bench.BOX_W, bench.BOX_H, bench.RMAX, bench.SEED)
     assert _overlapping_pairs(circles) > 1000  # the overlap branch of the pair operator is exercised
-    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
-        assert h.engine() == eb.ENGINE_PACKING
-        for k in range(5):  # sweep 1 from the seeded start, then free-running
-            h.iterate(1)
-            h.download(pg.G)
-            orc.run(1, THREADS, trace=False)
-            d = _maxdiff(pg.G, orc.G)
-            assert d <= TOL_F32, f"sweep {k + 1}: max |diff| {d}"
-        orc.run(45, THREADS, trace=False)  # reference iterate 50
-        _copy_state(pg.G, orc.G)
-        h.upload(pg.G)
-        h.iterate(1)
-        h.download(pg.G)
-    orc.run(1, THREADS, trace=False)
-    d = _maxdiff(pg.G, orc.G)
-    assert d <= TOL_F32, f"teacher-forced from iterate 50: max |diff| {d}"
+    _free_running_z(pg, orc, 5, N)
+    orc.init(bench.SEED, bench.BOX_W, bench.BOX_H, bench.RMAX, RHO, RHO_R, ALPHA)
+    worst = _teacher_forced(pg, orc, [0, 1, 2, 3, 4, 50], N)
+    print(f"N={N}: teacher-forced worst max|diff| {worst:.2e}")
     pg.close()
     orc.close()
 
@@ -103,25 +134,10 @@ def test_configuration1_n2000():
     N = 2000
     pg, orc, circles = _pair(N, 1.0, 1.0, 0.05, 7)
     assert _overlapping_pairs(circles) > 1000
-    with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
-        for k in range(8):
-            h.iterate(1)
-            h.download(pg.G)
-            orc.run(1, THREADS, trace=False)
-            d = _maxdiff(pg.G, orc.G)
-            assert d <= TOL_F32, f"free-running sweep {k + 1}: max |diff| {d}"
-    done = 8
-    for k in (50, 500):
-        orc.run(k - done, THREADS, trace=False)
-        done = k
-        _copy_state(pg.G, orc.G)
-        with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
-            h.iterate(1)
-            h.download(pg.G)
-        orc.run(1, THREADS, trace=False)
-        done += 1
-        d = _maxdiff(pg.G, orc.G)
-        assert d <= TOL_F32, f"teacher-forced from iterate {k}: max |diff| {d}"
+    _free_running_z(pg, orc, 8, N)
+    orc.init(7, 1.0, 1.0, 0.05, RHO, RHO_R, ALPHA)
+    worst = _teacher_forced(pg, orc, [0, 1, 2, 3, 4, 5, 6, 7, 50, 500], N)
+    print(f"N={N}: teacher-forced worst max|diff| {worst:.2e}")
 
 
 @pytest.mark.parametrize("cluster,coop_min_n", [(2, 200), (1, 0)])
