@@ -25,7 +25,7 @@ OK, EINVAL, ENOMEM, ECUDA, EUNSUPPORTED_OP, EUNSUPPORTED_GRAPH, ENONFINITE, ETIM
     0, -1, -2, -3, -4, -5, -6, -7, -8)
 OP_UNKNOWN, OP_PAIR, OP_WALL, OP_RADIUS = 0, 1, 2, 3
 ENGINE_AUTO, ENGINE_PACKING, ENGINE_GENERIC_F64, ENGINE_GENERIC_F32 = 0, 1, 2, 3
-SCHEDULE_AUTO, SCHEDULE_GRID, SCHEDULE_INSTANCE = 0, 1, 2
+SCHEDULE_AUTO, SCHEDULE_GRID, SCHEDULE_INSTANCE, SCHEDULE_ONCHIP = 0, 1, 2, 3
 
 OP_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                     C.c_int, C.c_int, C.c_void_p)

@@ -31,6 +31,7 @@ CU_SOURCES = {
     "packing_kernels.cu": [],
     "generic_kernels.cu": ["-fmad=false"],
     "noalloc.cu": [],
+    "onchip_kernels.cu": [],
     "setmlp.cu": [],
     "userops.cu": [],
 }

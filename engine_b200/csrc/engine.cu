@@ -466,6 +466,90 @@ static void pk_set_instance_schedule(paradmm_gpu *h, int cluster, int coop_min_n
         cudaGetLastError();  // the queue keeps its previous order; still a valid permutation
 }
 
+// The cluster-resident schedule (onchip_kernels.cu): every instance's size
+// class (the smallest group of 2^c CTAs whose shared memory holds it), the
+// cluster size (16 CTAs where the device co-schedules such clusters, else
+// 8), and the split of the resident clusters into groups: each class gets
+// clusters in proportion to its share of the pair work (sum of N^2), largest
+// class first, and the clusters left over go to the smallest class (a group
+// also serves smaller classes once its own queue is empty).  Returns false,
+// with a reason, when some instance cannot run this way.
+static bool pk_onchip_plan(paradmm_gpu *h, std::string &why)
+{
+    PkHost &P = *h->pk;
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device) != cudaSuccess) {
+        cudaGetLastError();
+        why = "device attributes";
+        return false;
+    }
+    const int smem = std::min(optin, 232448) - 2048;  // room for the kernel's static shared memory
+    if (P.shard_n > 0) { why = "a shard of an instance"; return false; }
+    if (h->from_graph) { why = "a handle built from a host graph (its uploads are not held on chip)"; return false; }
+    int csize = 0, nclu = 0;
+    for (int c : {16, 8}) {
+        int n = 0;
+        if (pk_onchip_max_clusters(P.V, c, smem, &n) == cudaSuccess && n >= 1) { csize = c; nclu = n; break; }
+        cudaGetLastError();
+    }
+    if (csize == 0) { why = "no cluster of 8 CTAs with this much shared memory fits the device"; return false; }
+    int maxc = 0;
+    while ((1 << (maxc + 1)) <= csize) ++maxc;
+    std::vector<std::vector<int>> cls(OC_CLASSES);
+    std::vector<double> work(OC_CLASSES, 0.0);
+    for (int i = 0; i < P.n_inst; ++i) {
+        const PkInst &I = P.inst[i];
+        const PkCircle &C0 = P.circ[I.circle_base];
+        if (C0.wall_count > OC_MAX_WALLS || C0.rad_count != 1) {
+            why = "an instance has more than 4 walls per circle or not one radius factor per circle";
+            return false;
+        }
+        int c = 0;
+        while (c <= maxc && pk_onchip_bytes(I.N, 1 << c) > smem) ++c;
+        if (c > maxc) { why = "an instance is too large for one cluster's shared memory"; return false; }
+        cls[c].push_back(i);
+        work[c] += (double)I.N * I.N;
+    }
+    std::vector<int> q, qoff(OC_CLASSES + 1, 0);
+    for (int c = 0; c < OC_CLASSES; ++c) {
+        std::stable_sort(cls[c].begin(), cls[c].end(), [&](int a, int b) { return P.inst[a].N > P.inst[b].N; });
+        qoff[c] = (int)q.size();
+        q.insert(q.end(), cls[c].begin(), cls[c].end());
+    }
+    qoff[OC_CLASSES] = (int)q.size();
+    double total = 0.0;
+    for (double x : work) total += x;
+    std::vector<unsigned char> glog2;
+    for (int c = maxc; c >= 0; --c) {
+        if (cls[c].empty()) continue;
+        int want = (int)std::lround(nclu * work[c] / total);
+        if (want < 1) want = 1;
+        want = std::min(want, nclu - (int)glog2.size());
+        for (int n = 0; n < want; ++n) glog2.push_back((unsigned char)c);
+    }
+    int smallest = 0;
+    while (smallest < OC_CLASSES && cls[smallest].empty()) ++smallest;
+    while ((int)glog2.size() < nclu) glog2.push_back((unsigned char)std::min(smallest, maxc));
+    if (!P.d_oc_queue) {
+        if (dput(h, &P.d_oc_queue, q) != PARADMM_OK || dalloc(h, (void **)&P.d_oc_ctr, sizeof(unsigned) * OC_CLASSES) != PARADMM_OK ||
+            dput(h, &P.d_oc_glog2, glog2) != PARADMM_OK) {
+            why = "device memory";
+            return false;
+        }
+    } else {
+        cudaMemcpy(P.d_oc_queue, q.data(), sizeof(int) * q.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(P.d_oc_glog2, glog2.data(), glog2.size(), cudaMemcpyHostToDevice);
+    }
+    P.oc_csize = csize;
+    P.oc_clusters = nclu;
+    P.oc_smem = smem;
+    P.oc_args.queue = P.d_oc_queue;
+    for (int c = 0; c <= OC_CLASSES; ++c) P.oc_args.qoff[c] = qoff[c];
+    P.oc_args.ctr = P.d_oc_ctr;
+    P.oc_args.glog2 = P.d_oc_glog2;
+    return true;
+}
+
 static int pk_finalize_build(paradmm_gpu *h)
 {
     PkHost &P = *h->pk;
@@ -575,6 +659,13 @@ static int pk_finalize_build(paradmm_gpu *h)
         std::stable_sort(P.order.begin(), P.order.end(), [&](int a, int b) { return P.inst[a].N > P.inst[b].N; });
         if ((rc = dput(h, &P.d_order, P.order))) return rc;
         pk_set_instance_schedule(h, h->opts.cluster_size, h->opts.reserved[0]);
+        if (req == PARADMM_SCHEDULE_ONCHIP) {
+            std::string why;
+            if (!pk_onchip_plan(h, why))
+                return pdm_set_error(PARADMM_EUNSUPPORTED_GRAPH, "the cluster-resident schedule cannot run this batch: %s",
+                                     why.c_str());
+            P.schedule = PARADMM_SCHEDULE_ONCHIP;
+        }
     }
     P.upload_iter.assign(P.n_inst, 0);
     P.age.assign(P.n_inst, 0);
@@ -928,8 +1019,14 @@ static int pk_enqueue_instances(paradmm_gpu *h, const PkRun &R, bool capturing)
     PDM_CUDA(cudaMemcpyAsync(P.D.status, P.h_status, sizeof(PkStatus) * P.n_inst, cudaMemcpyHostToDevice, h->stream));
     PDM_CUDA(cudaMemsetAsync(h->ctl, 0, sizeof(DevCtl), h->stream));
     PDM_CUDA(cudaEventRecordWithFlags(h->ev0, h->stream, evflags));
-    cudaError_t e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, P.n_early, &h->ctl->item_ctr[0],
-                                        P.inst_grid, P.cluster, h->stream);
+    cudaError_t e;
+    if (P.schedule == PARADMM_SCHEDULE_ONCHIP) {
+        PDM_CUDA(cudaMemsetAsync(P.d_oc_ctr, 0, sizeof(unsigned) * OC_CLASSES, h->stream));
+        e = pk_launch_onchip(P.V, P.D, R, P.oc_args, P.oc_clusters, P.oc_csize, P.oc_smem, h->stream);
+    } else {
+        e = pk_launch_instances(P.V, P.stream_hint, P.D, R, P.d_order, P.n_coop, P.n_early, &h->ctl->item_ctr[0],
+                                P.inst_grid, P.cluster, h->stream);
+    }
     if (e != cudaSuccess) return pdm_cuda_fail(e, "per-instance packing launch", __FILE__, __LINE__);
     PDM_CUDA(cudaEventRecordWithFlags(h->ev1, h->stream, evflags));
     PDM_CUDA(cudaMemcpyAsync(P.h_status, P.D.status, sizeof(PkStatus) * P.n_inst, cudaMemcpyDeviceToHost, h->stream));
@@ -981,6 +1078,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     key.bal_mu = R.bal_mu;
     key.bal_lmin = R.bal_lmin;
     key.bal_lmax = R.bal_lmax;
+    key.schedule = P.schedule;
     key.n_iter = R.n_iter;
     key.tol = tol;
     key.check_every = R.check_every;
@@ -1044,7 +1142,8 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
 {
     PkHost &P = *h->pk;
     std::fill(P.iters_last_call.begin(), P.iters_last_call.end(), 0LL);
-    if (P.schedule == PARADMM_SCHEDULE_INSTANCE) return pk_run_instances(h, n, tol, check_every, ms);
+    if (P.schedule == PARADMM_SCHEDULE_INSTANCE || P.schedule == PARADMM_SCHEDULE_ONCHIP)
+        return pk_run_instances(h, n, tol, check_every, ms);
     std::vector<char> done(P.n_inst, 0);
     double total_ms = 0;
     long long left = n;
@@ -1563,7 +1662,8 @@ extern "C" int paradmm_gpu_instance_times(const paradmm_gpu *h, double *begin_ms
     ok_status();
     if (!h || !h->pk || !begin_ms || !end_ms) return pdm_set_error(PARADMM_EINVAL, "needs a packing handle");
     const PkHost &P = *h->pk;
-    if (P.schedule != PARADMM_SCHEDULE_INSTANCE) return pdm_set_error(PARADMM_EINVAL, "instance times need the per-instance schedule");
+    if (P.schedule != PARADMM_SCHEDULE_INSTANCE && P.schedule != PARADMM_SCHEDULE_ONCHIP)
+        return pdm_set_error(PARADMM_EINVAL, "instance times need a per-instance schedule");
     unsigned long long t0 = ~0ull;
     for (const PkStatus &s : P.status) if (s.t_begin_ns && s.t_begin_ns < t0) t0 = s.t_begin_ns;
     for (int i = 0; i < P.n_inst; ++i) {
@@ -1824,6 +1924,9 @@ extern "C" int paradmm_gpu_autotune(paradmm_gpu *h, int sweeps, double tol, para
         for (int cl : {2, 4})
             for (int coop : {120, 200, 300})
                 if (maxN >= coop) cand.push_back({PARADMM_SCHEDULE_INSTANCE, cl, coop, 0});
+        std::string why;
+        if (P.schedule == PARADMM_SCHEDULE_ONCHIP || pk_onchip_plan(h, why)) cand.push_back({PARADMM_SCHEDULE_ONCHIP, 0, 0, 0});
+        else cudaGetLastError();
     }
     const int saved_schedule = P.schedule, saved_cluster = P.cluster, saved_coop = P.coop_min_n;
     const int saved_fallback = P.fallback_after;
@@ -1962,8 +2065,8 @@ extern "C" int paradmm_gpu_set_fallback(paradmm_gpu *h, int64_t after_sweeps)
     if (!h) return pdm_set_error(PARADMM_EINVAL, "handle is NULL");
     if (!h->pk) return pdm_set_error(PARADMM_EINVAL, "not a packing handle");
     if (after_sweeps < 0 || after_sweeps > INT_MAX) return pdm_set_error(PARADMM_EINVAL, "after_sweeps out of range");
-    if (after_sweeps > 0 && h->pk->schedule != PARADMM_SCHEDULE_INSTANCE)
-        return pdm_set_error(PARADMM_EINVAL, "the in-call fallback needs the per-instance schedule");
+    if (after_sweeps > 0 && h->pk->schedule != PARADMM_SCHEDULE_INSTANCE && h->pk->schedule != PARADMM_SCHEDULE_ONCHIP)
+        return pdm_set_error(PARADMM_EINVAL, "the in-call fallback needs a per-instance schedule");
     h->pk->fallback_after = (int)after_sweeps;
     return PARADMM_OK;
 }

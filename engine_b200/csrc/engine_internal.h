@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "generic.cuh"
 #include "packing.cuh"
+#include "packing_launch.h"
 
 int pdm_set_error(int status, const char *fmt, ...);
 void pdm_clear_status();  // marks the calling thread's last call as successful
@@ -34,6 +35,7 @@ struct PkGraphKey {
     int check_every, fallback_after, prof, cluster, n_coop, inst_grid, n_early;
     int bal_period, bal_lmin, bal_lmax;
     double bal_mu;
+    int schedule;
 };
 
 struct PkHost {
@@ -72,6 +74,12 @@ struct PkHost {
     int coop_min_n = 0;              // instances with N >= this are solved by a whole cluster
     int n_coop = 0;                  // how many instances that is (the first n_coop of the order)
     int n_early = 0;                 // clusters that start on the on-chip-solver instances (after the coop part of the order)
+    // cluster-resident schedule (PARADMM_SCHEDULE_ONCHIP)
+    int oc_csize = 0, oc_clusters = 0, oc_smem = 0;
+    int *d_oc_queue = nullptr;
+    unsigned *d_oc_ctr = nullptr;
+    unsigned char *d_oc_glog2 = nullptr;
+    OcArgs oc_args{};
     std::vector<int> order;          // instances, largest first (per-instance schedule)
     int *d_order = nullptr;          // the same on the device
     int prof = 0;                    // per-phase timing requested

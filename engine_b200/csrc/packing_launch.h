@@ -25,3 +25,19 @@ cudaError_t pk_launch_shard_begin(int V, bool stream_hint, const PkDev &D, const
                                   int row_lo, int row_hi, double4 *exch, cudaStream_t s);
 cudaError_t pk_launch_shard_end(int V, const PkDev &D, const PkRun &R, long long k, int nb, const double4 *exch,
                                 unsigned *done, cudaStream_t s);
+
+// Cluster-resident solver (onchip_kernels.cu).  Instances of size class c
+// need a group of 2^c CTAs (c = 0 .. OC_CLASSES - 1).
+#define OC_MAX_WALLS 4    // walls per circle the solver holds on chip
+#define OC_MAX_GROUP 16   // CTAs of the largest group (one whole cluster)
+#define OC_CLASSES 5      // group sizes 1, 2, 4, 8, 16
+struct OcArgs {
+    const int *queue;              // instances by class, each class largest first
+    int qoff[OC_CLASSES + 1];      // class c is queue[qoff[c] .. qoff[c + 1])
+    unsigned *ctr;                 // [OC_CLASSES] grab counters, zeroed before each launch
+    const unsigned char *glog2;    // per cluster: log2 of its group size
+};
+long long pk_onchip_bytes(int n_circles, int group);
+cudaError_t pk_onchip_max_clusters(int V, int csize, int smem, int *clusters);
+cudaError_t pk_launch_onchip(int V, const PkDev &D, const PkRun &R, const OcArgs &A, int n_clusters, int csize,
+                             int smem, cudaStream_t s);

@@ -84,7 +84,10 @@ typedef struct paradmm_gpu_opts {
 enum {
     PARADMM_SCHEDULE_AUTO = 0,     /* per-instance CTAs for batches of small instances, else grid-wide */
     PARADMM_SCHEDULE_GRID = 1,     /* every CTA works on every instance; grid barrier per sweep        */
-    PARADMM_SCHEDULE_INSTANCE = 2  /* one CTA per instance at a time, no grid barrier (N <= 1024)      */
+    PARADMM_SCHEDULE_INSTANCE = 2, /* one CTA per instance at a time, no grid barrier (N <= 1024)      */
+    PARADMM_SCHEDULE_ONCHIP = 3    /* per instance, its whole state held in the shared memory of a
+                                      group of 1-16 CTAs of a thread-block cluster for the solve
+                                      (instances up to ~450 circles, <= 4 walls per circle)          */
 };
 
 typedef struct paradmm_stats {

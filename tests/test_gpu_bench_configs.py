@@ -140,18 +140,22 @@ def test_configuration1_n2000():
     print(f"N={N}: teacher-forced worst max|diff| {worst:.2e}")
 
 
-@pytest.mark.parametrize("cluster,coop_min_n", [(2, 200), (1, 0)])
-def test_batched_instances_teacher_forced_inside_the_batch(cluster, coop_min_n):
+@pytest.mark.parametrize("schedule,cluster,coop_min_n", [(eb.SCHEDULE_INSTANCE, 2, 200), (eb.SCHEDULE_INSTANCE, 1, 0),
+                                                       (eb.SCHEDULE_ONCHIP, 0, 0)])
+def test_batched_instances_teacher_forced_inside_the_batch(schedule, cluster, coop_min_n):
     """Instances of the time-to-residual batch (seed 900000), picked to cover
-    the on-chip solver (N <= 40), single CTAs and whole clusters, set to
-    reference iterates k in {0, 40, 300} inside the 512-instance handle."""
+    the small-instance solver (N <= 40), single CTAs and whole clusters of the
+    tiled per-instance schedule, and every group size of the cluster-resident
+    one, set to reference iterates k in {0, 40, 300} inside the 512-instance
+    handle."""
     from engine_b200 import learned
     inst = learned.make_instances(512, 900000)
     sizes = np.array([d["n_circles"] for d in inst])
     picks = [int(np.argmin(sizes)), int(np.argmin(np.abs(sizes - 37))), int(np.argmin(np.abs(sizes - 120))),
-             int(np.argmin(np.abs(sizes - 199))), int(np.argmin(np.abs(sizes - 260))), int(np.argmax(sizes))]
+             int(np.argmin(np.abs(sizes - 150))), int(np.argmin(np.abs(sizes - 199))),
+             int(np.argmin(np.abs(sizes - 260))), int(np.argmin(np.abs(sizes - 330))), int(np.argmax(sizes))]
     picks = list(dict.fromkeys(picks))
-    b = learned.Batch(inst, device=0, schedule=eb.SCHEDULE_INSTANCE, cluster=cluster, coop_min_n=coop_min_n)
+    b = learned.Batch(inst, device=0, schedule=schedule, cluster=cluster, coop_min_n=coop_min_n)
     h = eb.Handle(b.h.value, b.lib)
     try:
         orcs = {}
