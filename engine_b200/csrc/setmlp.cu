@@ -15,8 +15,9 @@
 // Output: cx = cx0 + s o0, cy = cy0 + s o1, r = s max(o2, 0).
 // Training: mean squared error against converged packings produced by the
 // plain solver, Adam on FP32 master weights, BF16 copies for the GEMMs.
-// Every kernel here is this file's own (tiled FP32-accumulate GEMM with
-// BF16 weights, segment mean/sum, fused epilogues, Adam).
+// Every kernel here is this file's own (tensor-core GEMM with TF32 inputs,
+// BF16 weights and FP32 accumulation, segment mean/sum, fused epilogues,
+// Adam).
 #include <cuda_bf16.h>
 #include <stdio.h>
 #include <string.h>
@@ -107,10 +108,14 @@ __global__ void sm_targets(const SmInst *inst, int n_inst, const double *init, c
 }
 
 // ---------------------------------------------------------------------------
-// GEMM: C[M x N] = op(A) op(B) (+ C), FP32 accumulate.  A is FP32 [M][K]
-// (or [K][M] when TA), B is T [K][N] (or [N][K] when TB), T = float or bf16.
-// 64 x 64 tiles, K in chunks of 16, 256 threads, 4 x 4 outputs per thread.
-// split > 1 splits K over blockIdx.z and accumulates with atomics.
+// GEMM on the tensor cores: C[M x N] = op(A) op(B) (+ C) with TF32 inputs and
+// FP32 accumulation (mma.sync m16n8k8).  A is FP32 [M][K] (or [K][M] when
+// TA), B is T [K][N] (or [N][K] when TB), T = float or bf16; BF16 weights are
+// exact in TF32, FP32 activations are rounded to TF32 (10-bit mantissa).
+// 64 x 64 block tiles, K in chunks of 16, 4 warps of 32 x 32 (2 x 4 mma
+// tiles each).  split > 1 splits K over blockIdx.z: every split writes its
+// partial tile to its own slice of the workspace and sm_gemm_reduce adds the
+// slices in order, so the result does not depend on timing.
 // ---------------------------------------------------------------------------
 template <typename TB>
 PDM_D float ld_b(const TB *p);
@@ -119,61 +124,117 @@ PDM_D float ld_b<float>(const float *p) { return *p; }
 template <>
 PDM_D float ld_b<__nv_bfloat16>(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
 
-template <bool TA, bool TB, typename BT>
-__global__ void __launch_bounds__(256) sm_gemm(int M, int N, int K, const float *A, int lda, const BT *B, int ldb,
-                                               float *C, int ldc, int accumulate, int split)
+PDM_D unsigned to_tf32(float x)
 {
-    __shared__ float As[16][64 + 4];
-    __shared__ float Bs[16][64 + 4];
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+PDM_D void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2])
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+#define SM_KC 16       // K chunk
+#define SM_LD (SM_KC + 4)  // padded row of the staged tiles (conflict-free fragment loads)
+
+template <bool TA, bool TB, typename BT>
+__global__ void __launch_bounds__(128) sm_gemm_tc(int M, int N, int K, const float *A, int lda, const BT *B, int ldb,
+                                                  float *C, int ldc, int accumulate, int split, float *ws)
+{
+    __shared__ float As[64][SM_LD];  // [m][k]
+    __shared__ float Bs[64][SM_LD];  // [n][k]
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int wm = (w >> 1) * 32, wn = (w & 1) * 32;
     const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
     const int kper = (K + split - 1) / split;
     const int kbeg = blockIdx.z * kper, kend = min(K, kbeg + kper);
-    float acc[4][4] = {};
-    for (int k0 = kbeg; k0 < kend; k0 += 16) {
-        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
-            const int kk = e / 64, mm = e % 64;
+    float acc[2][4][4] = {};
+    for (int k0 = kbeg; k0 < kend; k0 += SM_KC) {
+        for (int e = tid; e < 64 * SM_KC; e += 128) {
+            int mm, kk;
+            if (TA) { kk = e / 64; mm = e % 64; } else { mm = e / SM_KC; kk = e % SM_KC; }  // coalesced along memory
             const int gm = m0 + mm, gk = k0 + kk;
-            float a = 0.f;
-            if (gm < M && gk < kend) a = TA ? A[(long long)gk * lda + gm] : A[(long long)gm * lda + gk];
-            As[kk][mm] = a;
-            const int gn = n0 + mm;
-            float bv = 0.f;
-            if (gn < N && gk < kend) bv = TB ? ld_b<BT>(B + (long long)gn * ldb + gk) : ld_b<BT>(B + (long long)gk * ldb + gn);
-            Bs[kk][mm] = bv;
+            As[mm][kk] = (gm < M && gk < kend) ? (TA ? A[(long long)gk * lda + gm] : A[(long long)gm * lda + gk]) : 0.f;
+        }
+        for (int e = tid; e < 64 * SM_KC; e += 128) {
+            int nn, kk;
+            if (TB) { nn = e / SM_KC; kk = e % SM_KC; } else { kk = e / 64; nn = e % 64; }
+            const int gn = n0 + nn, gk = k0 + kk;
+            Bs[nn][kk] = (gn < N && gk < kend) ? (TB ? ld_b<BT>(B + (long long)gn * ldb + gk) : ld_b<BT>(B + (long long)gk * ldb + gn))
+                                               : 0.f;
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            float a[4], b[4];
+        for (int ks = 0; ks < SM_KC; ks += 8) {
+            unsigned af[2][4], bf[4][2];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) { a[q] = As[kk][ty * 4 + q]; b[q] = Bs[kk][tx * 4 + q]; }
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + i * 16 + gid;
+                af[i][0] = to_tf32(As[r][ks + tig]);
+                af[i][1] = to_tf32(As[r + 8][ks + tig]);
+                af[i][2] = to_tf32(As[r][ks + tig + 4]);
+                af[i][3] = to_tf32(As[r + 8][ks + tig + 4]);
+            }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) {
+                const int c = wn + j * 8 + gid;
+                bf[j][0] = to_tf32(Bs[c][ks + tig]);
+                bf[j][1] = to_tf32(Bs[c][ks + tig + 4]);
+            }
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_tf32(acc[i][j], af[i], bf[j]);
         }
         __syncthreads();
     }
+    // epilogue: element (r, c) of mma tile (i, j) is acc[i][j][q] with
+    // r = gid (+ 8 for q >= 2), c = 2 tig + (q & 1)
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
-            if (gm < M && gn < N) {
-                float *c = C + (long long)gm * ldc + gn;
-                if (split > 1) atomicAdd(c, acc[i][j]);
-                else *c = accumulate ? *c + acc[i][j] : acc[i][j];
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int gm = m0 + wm + i * 16 + gid + (q >= 2 ? 8 : 0);
+                const int gn = n0 + wn + j * 8 + 2 * tig + (q & 1);
+                if (gm >= M || gn >= N) continue;
+                if (split > 1) ws[((long long)blockIdx.z * M + gm) * N + gn] = acc[i][j][q];
+                else {
+                    float *c = C + (long long)gm * ldc + gn;
+                    *c = accumulate ? *c + acc[i][j][q] : acc[i][j][q];
+                }
             }
-        }
 }
+
+// C[M x N] (+)= sum over the split slices of the workspace, in slice order.
+__global__ void sm_gemm_reduce(int M, int N, int split, const float *ws, float *C, int ldc, int accumulate)
+{
+    const long long n = (long long)M * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int z = 0; z < split; ++z) s += ws[z * n + e];
+        float *c = C + (e / N) * ldc + e % N;
+        *c = accumulate ? *c + s : s;
+    }
+}
+
+#define SM_WS_FLOATS (64LL * SM_H * SM_H)  // split-K workspace: up to 64 slices of a 128 x 128 product
 
 template <bool TA, bool TB, typename BT>
 static void gemm(cudaStream_t s, int M, int N, int K, const float *A, int lda, const BT *B, int ldb, float *C, int ldc,
-                 bool accumulate, int split = 1)
+                 bool accumulate, int split = 1, float *ws = nullptr)
 {
+    if (split > 1 && (!ws || (long long)split * M * N > SM_WS_FLOATS)) split = 1;
     dim3 grid((N + 63) / 64, (M + 63) / 64, split);
-    sm_gemm<TA, TB, BT><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, accumulate ? 1 : 0, split);
+    sm_gemm_tc<TA, TB, BT><<<grid, 128, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, accumulate ? 1 : 0, split, ws);
+    if (split > 1) sm_gemm_reduce<<<64, 256, 0, s>>>(M, N, split, ws, C, ldc, accumulate ? 1 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -287,6 +348,7 @@ struct paradmm_setmlp {
     float *H1 = nullptr, *H2 = nullptr, *O = nullptr, *dO = nullptr, *dH1 = nullptr, *dH2 = nullptr;
     float *G = nullptr, *P = nullptr, *dP = nullptr, *dG = nullptr;
     double *d_loss = nullptr;
+    float *ws = nullptr;             // split-K workspace of the weight-gradient GEMMs
     std::vector<void *> allocs;
 };
 
@@ -353,12 +415,12 @@ static void sm_backward(paradmm_setmlp *n, long long r0, long long rows, int b0,
     const int blocks = 148 * 4;
     const int split = std::max(1, std::min(64, M / 512));
     // layer 3
-    gemm<true, false>(s, SM_O, SM_H, M, n->dO, SM_O, n->H2, SM_H, n->g + SM_W3, SM_H, true, split);
+    gemm<true, false>(s, SM_O, SM_H, M, n->dO, SM_O, n->H2, SM_H, n->g + SM_W3, SM_H, true, split, n->ws);
     sm_colsum<<<SM_O, 256, 0, s>>>(n->dO, M, SM_O, n->g + SM_B3);
     gemm<false, false>(s, M, SM_H, SM_O, n->dO, SM_O, W3, SM_H, n->dH2, SM_H, false);
     sm_relu_back<<<blocks, 256, 0, s>>>(n->dH2, n->H2, M, SM_H, nullptr, nullptr, nullptr, 0);
     // layer 2
-    gemm<true, false>(s, SM_H, SM_H, M, n->dH2, SM_H, n->H1, SM_H, n->g + SM_W2, 2 * SM_H, true, split);
+    gemm<true, false>(s, SM_H, SM_H, M, n->dH2, SM_H, n->H1, SM_H, n->g + SM_W2, 2 * SM_H, true, split, n->ws);
     sm_colsum<<<SM_H, 256, 0, s>>>(n->dH2, M, SM_H, n->g + SM_B2);
     // dP = per-instance sums of dH2; dW2b += dP^T G; dG = dP W2b
     sm_seg_mean<<<std::min(nb, 1024), 128, 0, s>>>(n->dH2, SM_H, n->d_row0 + b0, n->d_nrows + b0, nb, n->dP, 0, (int)r0);
@@ -367,7 +429,7 @@ static void sm_backward(paradmm_setmlp *n, long long r0, long long rows, int b0,
     gemm<false, false>(s, M, SM_H, SM_H, n->dH2, SM_H, W2, 2 * SM_H, n->dH1, SM_H, false);
     sm_relu_back<<<blocks, 256, 0, s>>>(n->dH1, n->H1, M, SM_H, n->dG, n->d_row_inst + r0, n->d_nrows, b0);
     // layer 1
-    gemm<true, false>(s, SM_H, SM_F, M, n->dH1, SM_H, F, SM_F, n->g + SM_W1, SM_F, true, split);
+    gemm<true, false>(s, SM_H, SM_F, M, n->dH1, SM_H, F, SM_F, n->g + SM_W1, SM_F, true, split, n->ws);
     sm_colsum<<<SM_H, 256, 0, s>>>(n->dH1, M, SM_H, n->g + SM_B1);
 }
 
@@ -398,6 +460,7 @@ extern "C" int paradmm_setmlp_create(int device, uint64_t seed, paradmm_setmlp *
     if (!rc) rc = sm_alloc(n, (void **)&n->m2, sizeof(float) * SM_NPARAM);
     if (!rc) rc = sm_alloc(n, (void **)&n->pb, sizeof(__nv_bfloat16) * SM_NPARAM);
     if (!rc) rc = sm_alloc(n, (void **)&n->d_loss, sizeof(double));
+    if (!rc) rc = sm_alloc(n, (void **)&n->ws, sizeof(float) * SM_WS_FLOATS);
     if (rc) { paradmm_setmlp_destroy(n); return rc; }
     // He-style init from a splitmix64 stream (host), zero biases
     std::vector<float> h(SM_NPARAM, 0.f);
