@@ -337,7 +337,8 @@ def run_ttr(local: int, world: int = 1, rank: int = 0):
                         f"seeded Gaussian-code plain starts (seed {TTR_SEED})",
             "tol": TTR_TOL, "maxiter": TTR_MAXITER, "learned_budget": TTR_BUDGET,
             "ranks": world, "split": "instances dealt over the ranks by size (snake order), no communication",
-            "schedule": {"schedule": "instance" if tune["schedule"] == 2 else "grid", "block_width": tune["block_width"],
+            "schedule": {"schedule": {1: "grid", 2: "instance", 3: "onchip"}.get(tune["schedule"], str(tune["schedule"])),
+                         "block_width": tune["block_width"],
                          "cluster": tune["cluster_size"],
                          "coop_min_n": tune["coop_min_n"], "autotune_candidates": tune["candidates"],
                          "probe_ms_best": tune["ms"], "probe_ms_worst": tune["worst_ms"]},

@@ -677,6 +677,16 @@ static int pk_finalize_build(paradmm_gpu *h)
     return PARADMM_OK;
 }
 
+// Whether a launch must read the penalty scale: balancing on, or some
+// instance still at a scale other than 1 (or with a change pending).
+static int pk_bal_any(const PkHost &P)
+{
+    if (P.bal_period > 0) return 1;
+    for (const PkStatus &s : P.status)
+        if (s.bal_pass_age > 0 || s.bal_log2_cur != 0 || s.bal_log2_new != 0) return 1;
+    return 0;
+}
+
 // Instance i's state was just set (create, warm start, upload): balancing
 // ages restart, the penalty scale returns to 1.
 static void pk_state_set(PkHost &P, int i)
@@ -1072,6 +1082,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     R.bal_mu = P.bal_mu;
     R.bal_lmin = P.bal_lmin;
     R.bal_lmax = P.bal_lmax;
+    R.bal_any = pk_bal_any(P);
     PkGraphKey key;
     memset(&key, 0, sizeof key);
     key.bal_period = R.bal_period;
@@ -1079,6 +1090,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     key.bal_lmin = R.bal_lmin;
     key.bal_lmax = R.bal_lmax;
     key.schedule = P.schedule;
+    key.bal_any = R.bal_any;
     key.n_iter = R.n_iter;
     key.tol = tol;
     key.check_every = R.check_every;
@@ -1184,6 +1196,7 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
         R.bal_mu = P.bal_mu;
         R.bal_lmin = P.bal_lmin;
         R.bal_lmax = P.bal_lmax;
+    R.bal_any = pk_bal_any(P);
         PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
         cudaError_t e = pk_launch_persistent(P.V, P.stream_hint, P.D, R, P.grid, h->stream);
         if (e != cudaSuccess) return pdm_cuda_fail(e, "packing persistent launch", __FILE__, __LINE__);
@@ -2249,6 +2262,11 @@ extern "C" int paradmm_gpu_shard_begin(paradmm_gpu *h, void *exchange, void *str
     R.dynamic = 1;
     R.tol = P.shard_tol;
     R.check_every = P.shard_check_every;
+    R.bal_period = P.bal_period;
+    R.bal_mu = P.bal_mu;
+    R.bal_lmin = P.bal_lmin;
+    R.bal_lmax = P.bal_lmax;
+    R.bal_any = pk_bal_any(P);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = pk_launch_shard_begin(P.V, P.stream_hint, P.D, R, P.grid, P.inst[0].nb, P.row_lo, P.row_hi,
                                           (double4 *)exchange, s);
@@ -2278,6 +2296,7 @@ extern "C" int paradmm_gpu_shard_end(paradmm_gpu *h, const void *exchange, void 
     R.bal_mu = P.bal_mu;
     R.bal_lmin = P.bal_lmin;
     R.bal_lmax = P.bal_lmax;
+    R.bal_any = pk_bal_any(P);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = pk_launch_shard_end(P.V, P.D, R, P.shard_k, P.inst[0].nb, (const double4 *)exchange, P.d_done, s);
     if (e != cudaSuccess) return pdm_cuda_fail(e, "shard consensus launch", __FILE__, __LINE__);

@@ -35,7 +35,7 @@ struct PkGraphKey {
     int check_every, fallback_after, prof, cluster, n_coop, inst_grid, n_early;
     int bal_period, bal_lmin, bal_lmax;
     double bal_mu;
-    int schedule;
+    int schedule, bal_any;
 };
 
 struct PkHost {

@@ -242,7 +242,7 @@ PDM_D void oc_solve(const PkDev &D, const PkRun &R, int i, const OcGroup &G, OcS
     long long k_sw = R.it0;
     for (; k_sw < R.it0 + R.n_iter; ++k_sw) {
         const bool zmode = k_sw == zmode_at;
-        const PkBal bal = pk_bal_at(st, k_sw);
+        const PkBal bal = R.bal_any ? pk_bal_at(st, k_sw) : pk_bal_none();
         // ---- pass: strips (warps)
         for (int ls = w; ls < ns; ls += OC_WARPS) {
             const int x = s0 + ls, t = x / OC_S, s = x % OC_S;
@@ -451,7 +451,9 @@ PDM_D void oc_solve(const PkDev &D, const PkRun &R, int i, const OcGroup &G, OcS
             check_from = k_sw + 2;
             bal_from = k_sw + 2;
             restart_at = -1;
-            __syncthreads();
+            // the leader's reset of the status (penalty scale included) reaches
+            // every CTA of the group before the next pass reads it
+            oc_group_sync(gs, D.ctl);
             continue;
         }
         if (stop) break;

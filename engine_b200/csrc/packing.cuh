@@ -166,6 +166,8 @@ struct PkRun {
     int bal_period;   // residual balancing: decide every bal_period iterates (0: off; >= 3)
     double bal_mu;    // ... double the penalties when r > mu s, halve them when s > mu r
     int bal_lmin, bal_lmax;  // ... within scales 2^bal_lmin .. 2^bal_lmax
+    int bal_any;      // balancing on, or some instance's penalties not at scale 1: passes read the scale
+    int pad3;
 };
 
 // Residual balancing of the penalties (no reference counterpart: the
@@ -184,6 +186,14 @@ struct PkBal {
     float uf;  // factor on U right after its update in this pass (1, 1/2 or 2)
     float rs;  // penalty scale of this pass's radius operator
 };
+
+PDM_D PkBal pk_bal_none()
+{
+    PkBal b;
+    b.uf = 1.0f;
+    b.rs = 1.0f;
+    return b;
+}
 
 PDM_D PkBal pk_bal_at(const PkStatus *st, long long k)
 {

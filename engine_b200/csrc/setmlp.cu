@@ -108,10 +108,12 @@ __global__ void sm_targets(const SmInst *inst, int n_inst, const double *init, c
 }
 
 // ---------------------------------------------------------------------------
-// GEMM on the tensor cores: C[M x N] = op(A) op(B) (+ C) with TF32 inputs and
-// FP32 accumulation (mma.sync m16n8k8).  A is FP32 [M][K] (or [K][M] when
-// TA), B is T [K][N] (or [N][K] when TB), T = float or bf16; BF16 weights are
-// exact in TF32, FP32 activations are rounded to TF32 (10-bit mantissa).
+// GEMM on the tensor cores: C[M x N] = op(A) op(B) (+ C) with FP32
+// accumulation (mma.sync m16n8k8, TF32 inputs).  A is FP32 [M][K] (or [K][M]
+// when TA), B is T [K][N] (or [N][K] when TB), T = float or bf16.  FP32
+// operands are split into two TF32 numbers (hi + lo) and the product is
+// taken as the sum of the two or three significant partial products, so the
+// result has FP32 accuracy; BF16 weights are exact in TF32.
 // 64 x 64 block tiles, K in chunks of 16, 4 warps of 32 x 32 (2 x 4 mma
 // tiles each).  split > 1 splits K over blockIdx.z: every split writes its
 // partial tile to its own slice of the workspace and sm_gemm_reduce adds the
@@ -129,6 +131,12 @@ PDM_D unsigned to_tf32(float x)
     unsigned r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return r;
+}
+
+PDM_D void split_tf32(float x, unsigned &hi, unsigned &lo)
+{
+    hi = to_tf32(x);
+    lo = to_tf32(x - __uint_as_float(hi));
 }
 
 PDM_D void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2])
@@ -152,6 +160,7 @@ __global__ void __launch_bounds__(128) sm_gemm_tc(int M, int N, int K, const flo
     const int gid = lane >> 2, tig = lane & 3;
     const int wm = (w >> 1) * 32, wn = (w & 1) * 32;
     const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    constexpr bool B_EXACT_TF32 = sizeof(BT) == 2;  // BF16 has 8 significand bits, TF32 11
     const int kper = (K + split - 1) / split;
     const int kbeg = blockIdx.z * kper, kend = min(K, kbeg + kper);
     float acc[2][4][4] = {};
@@ -172,25 +181,32 @@ __global__ void __launch_bounds__(128) sm_gemm_tc(int M, int N, int K, const flo
         __syncthreads();
 #pragma unroll
         for (int ks = 0; ks < SM_KC; ks += 8) {
-            unsigned af[2][4], bf[4][2];
+            // each operand as a sum of two TF32 numbers, hi + lo, so that the
+            // products keep FP32 accuracy: a_hi b + a_lo b when B is BF16 (exact
+            // in TF32), a_hi b_hi + a_hi b_lo + a_lo b_hi when B is FP32
+            unsigned ah[2][4], al[2][4], bh[4][2], bl[4][2];
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
                 const int r = wm + i * 16 + gid;
-                af[i][0] = to_tf32(As[r][ks + tig]);
-                af[i][1] = to_tf32(As[r + 8][ks + tig]);
-                af[i][2] = to_tf32(As[r][ks + tig + 4]);
-                af[i][3] = to_tf32(As[r + 8][ks + tig + 4]);
+                split_tf32(As[r][ks + tig], ah[i][0], al[i][0]);
+                split_tf32(As[r + 8][ks + tig], ah[i][1], al[i][1]);
+                split_tf32(As[r][ks + tig + 4], ah[i][2], al[i][2]);
+                split_tf32(As[r + 8][ks + tig + 4], ah[i][3], al[i][3]);
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int c = wn + j * 8 + gid;
-                bf[j][0] = to_tf32(Bs[c][ks + tig]);
-                bf[j][1] = to_tf32(Bs[c][ks + tig + 4]);
+                split_tf32(Bs[c][ks + tig], bh[j][0], bl[j][0]);
+                split_tf32(Bs[c][ks + tig + 4], bh[j][1], bl[j][1]);
             }
 #pragma unroll
             for (int i = 0; i < 2; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) mma_tf32(acc[i][j], af[i], bf[j]);
+                for (int j = 0; j < 4; ++j) {
+                    mma_tf32(acc[i][j], al[i], bh[j]);
+                    if (!B_EXACT_TF32) mma_tf32(acc[i][j], ah[i], bl[j]);
+                    mma_tf32(acc[i][j], ah[i], bh[j]);
+                }
         }
         __syncthreads();
     }
