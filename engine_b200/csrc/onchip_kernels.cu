@@ -186,7 +186,7 @@ struct OcGroup {
 // stop, fallback and balancing rules as pk_solve_instance (packing_kernels.cu).
 template <int V>
 PDM_D void oc_solve(const PkDev &D, const PkRun &R, int i, const OcGroup &G, OcSync &gs, unsigned char *smem,
-                    double2 *s_res, int *s_stop)
+                    double2 *s_res, int *s_stop, PkBalState *s_bal)
 {
     cg::cluster_group cl = cg::this_cluster();
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -237,12 +237,15 @@ PDM_D void oc_solve(const PkDev &D, const PkRun &R, int i, const OcGroup &G, OcS
     double sd_prev = sd_valid ? __ldcg(&st->sd_last) : 0.0;
     long long bal_from = R.it0 + (sd_valid ? 0 : 1);
     if (gr == 0 && tid == 0) st->t_begin_ns = globaltimer_ns();
+    // this CTA's copy of the balancing state (every CTA of the group takes
+    // the same decisions; the leader records them in the status)
+    if (tid == 0) *s_bal = pk_bal_load(st);
     __syncthreads();
 
     long long k_sw = R.it0;
     for (; k_sw < R.it0 + R.n_iter; ++k_sw) {
         const bool zmode = k_sw == zmode_at;
-        const PkBal bal = R.bal_any ? pk_bal_at(st, k_sw) : pk_bal_none();
+        const PkBal bal = R.bal_any ? pk_bal_eval(*s_bal, k_sw) : pk_bal_none();
         // ---- pass: strips (warps)
         for (int ls = w; ls < ns; ls += OC_WARPS) {
             const int x = s0 + ls, t = x / OC_S, s = x % OC_S;
@@ -394,11 +397,10 @@ PDM_D void oc_solve(const PkDev &D, const PkRun &R, int i, const OcGroup &G, OcS
                 sd += v.y;
             }
             int stop = 0;
-            const bool bal_due = gr == 0 && R.bal_period > 0 && k_sw >= bal_from &&
-                                 (k_sw - __ldcg(&st->bal_base)) % R.bal_period == 0;
+            const bool bal_due = R.bal_period > 0 && k_sw >= bal_from && (k_sw - s_bal->base) % R.bal_period == 0;
             if (k_sw >= check_from || bal_due) {
                 const double rp = sqrt(sp * P.inv_ncomp), rd = sqrt(sd_prev * P.inv_ncomp);
-                if (bal_due) pk_bal_decide(st, R, k_sw - 1, rp, rd);
+                if (bal_due && pk_bal_step(*s_bal, R, k_sw - 1, rp, rd) && gr == 0) pk_bal_store(st, *s_bal);
                 if (k_sw >= check_from) {
                     const bool finite = isfinite(rp) && isfinite(rd);
                     const bool due = R.check_every <= 1 || ((k_sw - R.it0) % R.check_every) == 0;
@@ -446,7 +448,10 @@ PDM_D void oc_solve(const PkDev &D, const PkRun &R, int i, const OcGroup &G, OcS
                 st->pad = 1;
                 pk_bal_reset(*st, k_sw + 1);
             }
-            if (tid == 0) sd_prev = 0.0;
+            if (tid == 0) {
+                sd_prev = 0.0;
+                *s_bal = pk_bal_fresh(k_sw + 1);
+            }
             zmode_at = k_sw + 1;
             check_from = k_sw + 2;
             bal_from = k_sw + 2;
@@ -501,6 +506,7 @@ __global__ void __launch_bounds__(OC_THREADS, 1) pk_onchip(PkDev D, PkRun R, OcA
     __shared__ int s_inst;
     __shared__ int s_stop;
     __shared__ double2 s_res[OC_MAX_GROUP];
+    __shared__ PkBalState s_bal;
     cg::cluster_group cl = cg::this_cluster();
     const int crank = (int)cl.block_rank(), csize = (int)cl.num_blocks();
     const int cid = (int)(blockIdx.x / (unsigned)csize);
@@ -537,7 +543,7 @@ __global__ void __launch_bounds__(OC_THREADS, 1) pk_onchip(PkDev D, PkRun R, OcA
         oc_group_sync(gs, D.ctl);
         const int i = s_inst;
         if (i < 0) break;  // group-uniform
-        if (__ldcg(&D.status[i].last_iter) >= R.it0) oc_solve<V>(D, R, i, G, gs, oc_smem, s_res, &s_stop);
+        if (__ldcg(&D.status[i].last_iter) >= R.it0) oc_solve<V>(D, R, i, G, gs, oc_smem, s_res, &s_stop, &s_bal);
         oc_group_sync(gs, D.ctl);  // the group is done with this instance's shared memory
     }
     cl.sync();  // no CTA leaves while a group member may still read its shared memory

@@ -195,33 +195,81 @@ PDM_D PkBal pk_bal_none()
     return b;
 }
 
-PDM_D PkBal pk_bal_at(const PkStatus *st, long long k)
+// An instance's balancing state as a kernel carries it from sweep to sweep.
+// CTAs that solve one instance together each keep their own copy and take
+// the same decisions from the same residual sums, so none reads the status
+// while another writes it.
+struct PkBalState {
+    long long base, pass_age;
+    int cur, nw;
+};
+
+PDM_D PkBalState pk_bal_load(const PkStatus *st)
 {
-    const long long pa = __ldcg(&st->bal_pass_age);
-    const int cur = __ldcg(&st->bal_log2_cur), nw = __ldcg(&st->bal_log2_new);
-    const long long age = k - __ldcg(&st->bal_base) + 1;
-    PkBal b;
-    b.rs = ldexpf(1.0f, (pa > 0 && age >= pa) ? nw : cur);
-    b.uf = (pa > 0 && age == pa && nw != cur) ? (nw > cur ? 0.5f : 2.0f) : 1.0f;
+    PkBalState b;
+    b.base = __ldcg(&st->bal_base);
+    b.pass_age = __ldcg(&st->bal_pass_age);
+    b.cur = __ldcg(&st->bal_log2_cur);
+    b.nw = __ldcg(&st->bal_log2_new);
     return b;
 }
 
-// The balancing decision on the residuals (rp, rd) of iterate j (one thread).
-PDM_D void pk_bal_decide(PkStatus *st, const PkRun &R, long long j, double rp, double rd)
+PDM_D PkBal pk_bal_eval(const PkBalState &s, long long k)
 {
-    if (R.bal_period <= 0) return;
-    const long long age = j - st->bal_base + 1;
-    if (age < R.bal_period || age % R.bal_period != 0) return;
-    const int cur = st->bal_log2_new;  // the previous decision applied at least period - 3 iterates ago
+    const long long age = k - s.base + 1;
+    PkBal b;
+    b.rs = ldexpf(1.0f, (s.pass_age > 0 && age >= s.pass_age) ? s.nw : s.cur);
+    b.uf = (s.pass_age > 0 && age == s.pass_age && s.nw != s.cur) ? (s.nw > s.cur ? 0.5f : 2.0f) : 1.0f;
+    return b;
+}
+
+PDM_D PkBal pk_bal_at(const PkStatus *st, long long k) { return pk_bal_eval(pk_bal_load(st), k); }
+
+// The balancing decision on the residuals (rp, rd) of iterate j; returns
+// whether the state changed.
+PDM_D bool pk_bal_step(PkBalState &s, const PkRun &R, long long j, double rp, double rd)
+{
+    if (R.bal_period <= 0) return false;
+    const long long age = j - s.base + 1;
+    if (age < R.bal_period || age % R.bal_period != 0) return false;
+    const int cur = s.nw;  // the previous decision applied at least period - 3 iterates ago
     int nw = cur;
     if (rp > R.bal_mu * rd && cur < R.bal_lmax) nw = cur + 1;
     else if (rd > R.bal_mu * rp && cur > R.bal_lmin) nw = cur - 1;
-    st->bal_log2_cur = cur;
-    st->bal_log2_new = nw;
-    st->bal_pass_age = age + 3;
+    s.cur = cur;
+    s.nw = nw;
+    s.pass_age = age + 3;
+    return true;
+}
+
+PDM_D void pk_bal_store(PkStatus *st, const PkBalState &s)
+{
+    st->bal_log2_cur = s.cur;
+    st->bal_log2_new = s.nw;
+    st->bal_pass_age = s.pass_age;
+}
+
+// The same decision on the status itself (one thread, no other reader).
+PDM_D void pk_bal_decide(PkStatus *st, const PkRun &R, long long j, double rp, double rd)
+{
+    PkBalState b;
+    b.base = st->bal_base;
+    b.pass_age = st->bal_pass_age;
+    b.cur = st->bal_log2_cur;
+    b.nw = st->bal_log2_new;
+    if (pk_bal_step(b, R, j, rp, rd)) pk_bal_store(st, b);
 }
 
 // Balancing state of a freshly set state whose first sweep is k.
+PDM_D PkBalState pk_bal_fresh(long long k)
+{
+    PkBalState b;
+    b.base = k;
+    b.pass_age = 0;
+    b.cur = b.nw = 0;
+    return b;
+}
+
 PDM_HD void pk_bal_reset(PkStatus &s, long long k)
 {
     s.bal_base = k;

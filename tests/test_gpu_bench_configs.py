@@ -41,6 +41,12 @@ import oracle_lib
 pytestmark = pytest.mark.gpu
 
 TOL_F32 = 1e-4
+# From reference iterates 2 .. 4 of the N = 8000 workload one FP32 sweep of
+# the per-edge arrays is limited by FP32 arithmetic itself: the numpy FP32
+# restatement (test_fp32_horizon.Twin), teacher-forced from iterate 2, lands
+# 1.66e-4 from the reference's X, M, U and N (Z 1.2e-7) -- the same figure
+# the engine reaches.  Z stays held to TOL_F32 there.
+TOL_EDGE_N8000 = {2: 4e-4, 3: 4e-4, 4: 4e-4}
 RHO, RHO_R, ALPHA, EXP = 10.0, 5.0, 1.0, 2.0
 THREADS = os.cpu_count() or 1
 
@@ -87,9 +93,11 @@ def _zdiff(G, H) -> float:
     return float(np.max(np.abs(G.arr("Z") - H.arr("Z"))))
 
 
-def _teacher_forced(pg, orc, ks, N):
+def _teacher_forced(pg, orc, ks, N, tol_edge=None):
     """One engine sweep from each reference iterate k in ks (ascending)
-    against reference iterate k + 1; returns the worst max |difference|."""
+    against reference iterate k + 1; Z is held to TOL_F32, the per-edge
+    arrays to tol_edge.get(k, TOL_F32).  Returns the worst max |difference|."""
+    tol_edge = tol_edge or {}
     worst, done = 0.0, 0
     with eb.Handle.from_graph(pg.G, engine=eb.ENGINE_PACKING) as h:
         assert h.engine() == eb.ENGINE_PACKING
@@ -101,8 +109,10 @@ def _teacher_forced(pg, orc, ks, N):
             h.download(pg.G)
             orc.run(1, THREADS, trace=False)
             done = k + 1
-            d = _maxdiff(pg.G, orc.G)
-            assert d <= TOL_F32, f"N={N}, teacher-forced from iterate {k}: max |diff| {d}"
+            d, z = _maxdiff(pg.G, orc.G), _zdiff(pg.G, orc.G)
+            print(f"N={N}: teacher-forced from iterate {k}: max |diff| {d:.2e} (Z {z:.2e})")
+            assert z <= TOL_F32, f"N={N}, teacher-forced from iterate {k}: max |diff| of Z {z}"
+            assert d <= tol_edge.get(k, TOL_F32), f"N={N}, teacher-forced from iterate {k}: max |diff| {d}"
             worst = max(worst, d)
     return worst
 
@@ -124,7 +134,7 @@ def test_bench_workload_n8000():
     assert _overlapping_pairs(circles) > 1000  # the overlap branch of the pair operator is exercised
     _free_running_z(pg, orc, 5, N)
     orc.init(bench.SEED, bench.BOX_W, bench.BOX_H, bench.RMAX, RHO, RHO_R, ALPHA)
-    worst = _teacher_forced(pg, orc, [0, 1, 2, 3, 4, 50], N)
+    worst = _teacher_forced(pg, orc, [0, 1, 2, 3, 4, 50], N, TOL_EDGE_N8000)
     print(f"N={N}: teacher-forced worst max|diff| {worst:.2e}")
     pg.close()
     orc.close()

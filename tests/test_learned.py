@@ -149,7 +149,8 @@ def test_trained_network_reduces_sweeps():
     """The committed weights on fresh instances of the batched workload
     (N uniform in [20, 400]): the learned warm start (with the in-launch
     fallback) needs fewer sweeps than the plain start, and the packings it
-    converges to are no smaller (total radius) and as feasible."""
+    converges to are no smaller (total radius) and as feasible (the per-instance
+    violations at the stopping rule, by quantile)."""
     from engine_b200 import learned
     inst = learned.make_instances(48, 4242)
     net = learned.SetMLP()
@@ -166,6 +167,14 @@ def test_trained_network_reduces_sweeps():
     tot_p = sum(c[:, 2].sum() for c in pl["circles"])
     tot_l = sum(c[:, 2].sum() for c in le["circles"])
     assert (tot_l - tot_p) / tot_p > -1e-3, (tot_l, tot_p)
-    vp = max(x["max_violation"] for x, c in zip(pl["stats"], conv_p) if c)
-    vl = max(x["max_violation"] for x, c in zip(le["stats"], conv_l) if c)
-    assert vl <= max(10 * vp, 1e-4), (vl, vp)
+    # feasibility at the same stopping rule (r + s <= 1e-5): the learned
+    # start's violations are distributed like the plain start's -- median and
+    # 90th percentile no worse than plain's (10 % slack for 48 instances), the
+    # worst instance within 1.5x of plain's worst
+    vp = np.array([x["max_violation"] for x, c in zip(pl["stats"], conv_p) if c])
+    vl = np.array([x["max_violation"] for x, c in zip(le["stats"], conv_l) if c])
+    qp, ql = np.quantile(vp, [0.5, 0.9]), np.quantile(vl, [0.5, 0.9])
+    print(f"violation median/p90/max: plain {qp[0]:.2e}/{qp[1]:.2e}/{vp.max():.2e}, "
+          f"learned {ql[0]:.2e}/{ql[1]:.2e}/{vl.max():.2e}")
+    assert np.all(ql <= 1.1 * qp + 1e-7), (ql, qp)
+    assert vl.max() <= 1.5 * vp.max() + 1e-7, (vl.max(), vp.max())
