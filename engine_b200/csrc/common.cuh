@@ -15,12 +15,11 @@
 enum : int {
     DEV_OK = 0,
     DEV_BARRIER_TIMEOUT = 1,
-    DEV_COPY_TIMEOUT = 2,
 };
 
 static inline const char *pdm_dev_err_name(int e)
 {
-    return e == DEV_BARRIER_TIMEOUT ? "grid barrier" : e == DEV_COPY_TIMEOUT ? "bulk copy completion" : "unknown";
+    return e == DEV_BARRIER_TIMEOUT ? "grid barrier" : "unknown";
 }
 
 // Control block of one persistent launch: grid barrier, error flag, work
@@ -116,63 +115,8 @@ PDM_D bool grid_barrier(DevCtl *ctl)
     return ok != 0;
 }
 
-// ----------------------------------------------------------------------------
-// Bulk asynchronous copies (TMA engine, no tensor map) into shared memory,
-// completed through an mbarrier with a transaction count.  Only copies from
-// this GPU's global memory into the issuing CTA's own shared memory are
-// issued here.
-// ----------------------------------------------------------------------------
+// Shared-memory address of a generic pointer into this CTA's shared memory.
 PDM_D unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-PDM_D void mbar_init(uint64_t *bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-// One arrival that also announces `bytes` of copies completing on this phase.
-PDM_D void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
-{
-    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-PDM_D bool mbar_try_wait(uint64_t *bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait for the phase of `bar` with the given parity.  A wait that
-// runs out records DEV_COPY_TIMEOUT (the launch then ends at its next grid
-// barrier) and returns false; the caller's data is not valid then.
-#define PDM_MBAR_MAX_POLLS (1u << 26)
-PDM_D bool mbar_wait(uint64_t *bar, unsigned parity, DevCtl *ctl)
-{
-    for (unsigned n = 0; n < PDM_MBAR_MAX_POLLS; ++n)
-        if (mbar_try_wait(bar, parity)) return true;
-    atomicCAS(&ctl->err, DEV_OK, DEV_COPY_TIMEOUT);
-    return false;
-}
-
-// Global -> shared bulk copy of `bytes` (a multiple of 16, both addresses
-// 16-byte aligned), completing on `bar`.
-PDM_D void bulk_load_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-// Orders this thread's earlier generic-proxy shared-memory accesses before
-// later async-proxy (bulk copy) accesses.
-PDM_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Loads/stores of data that other blocks of the same launch write: through
 // L2 only (the per-SM L1 is not coherent within a launch).
