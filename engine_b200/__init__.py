@@ -174,6 +174,12 @@ _SIGS = {
     "paradmm_gpu_shard_end": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "paradmm_gpu_shard_poll": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "paradmm_gpu_shard_finish": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Stats)]),
+    "paradmm_gpu_shard_fused_buffers": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "paradmm_gpu_shard_run_fused": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p),
+                                              C.POINTER(C.c_void_p), C.c_int, C.c_void_p]),
+    "paradmm_gpu_ipc_export": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "paradmm_gpu_ipc_import": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "paradmm_gpu_ipc_close": (C.c_int, [C.c_int, C.c_void_p]),
     "paradmm_last_status": (C.c_int, []),
     "paradmm_last_error_string": (C.c_char_p, []),
     "paradmm_set_sweep_options": (None, [C.POINTER(Opts)]),

@@ -15,11 +15,12 @@
 enum : int {
     DEV_OK = 0,
     DEV_BARRIER_TIMEOUT = 1,
+    DEV_PEER_TIMEOUT = 2,  // a rank's flag for a sweep did not arrive (sharded instance)
 };
 
 static inline const char *pdm_dev_err_name(int e)
 {
-    return e == DEV_BARRIER_TIMEOUT ? "grid barrier" : "unknown";
+    return e == DEV_BARRIER_TIMEOUT ? "grid barrier" : e == DEV_PEER_TIMEOUT ? "exchange with another rank" : "unknown";
 }
 
 // Control block of one persistent launch: grid barrier, error flag, work
@@ -71,7 +72,9 @@ PDM_D unsigned atom_add_acq_rel_u32(unsigned *p, unsigned v)
 
 PDM_D int ld_volatile_i32(const int *p) { return *(const volatile int *)p; }
 
-// Grid-wide barrier for a cooperative (co-resident) launch.  One counter
+// Barrier of `nblocks` co-resident blocks that share `ctl` (the whole grid of
+// a cooperative launch, or one rank's blocks of a launch that holds several
+// ranks).  One counter
 // that only grows within a launch (the host zeroes it): a block's arrival
 // returns its position, which fixes the count that ends this round (the next
 // multiple of the grid size), and the block waits until the counter reaches
@@ -81,12 +84,11 @@ PDM_D int ld_volatile_i32(const int *p) { return *(const volatile int *)p; }
 // PDM_BARRIER_TIMEOUT_NS) and PDM_BARRIER_MAX_POLLS; on timeout, or when
 // another block has already recorded an error, it returns false and the
 // caller leaves its loop.  All threads of the block get the same answer.
-PDM_D bool grid_barrier(DevCtl *ctl)
+PDM_D bool grid_barrier_n(DevCtl *ctl, unsigned nblocks)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
         __threadfence();
         const unsigned pos = atom_add_acq_rel_u32(&ctl->bar_count, 1u);
         const unsigned target = (pos / nblocks + 1u) * nblocks;
@@ -113,6 +115,22 @@ PDM_D bool grid_barrier(DevCtl *ctl)
     const int ok = s_ok;
     __syncthreads();
     return ok != 0;
+}
+
+// The barrier over every block of the launch.
+PDM_D bool grid_barrier(DevCtl *ctl) { return grid_barrier_n(ctl, gridDim.x * gridDim.y * gridDim.z); }
+
+// System-scope flag accesses (flags another GPU writes or reads over NVLink).
+PDM_D unsigned long long ld_acquire_sys_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+PDM_D void st_release_sys_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // Shared-memory address of a generic pointer into this CTA's shared memory.

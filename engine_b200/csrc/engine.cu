@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstddef>
 #include <cmath>
 #include <mutex>
 #include <thread>
@@ -1937,9 +1938,9 @@ extern "C" int paradmm_gpu_autotune(paradmm_gpu *h, int sweeps, double tol, para
         for (int cl : {2, 4})
             for (int coop : {120, 200, 300})
                 if (maxN >= coop) cand.push_back({PARADMM_SCHEDULE_INSTANCE, cl, coop, 0});
-        std::string why;
-        if (P.schedule == PARADMM_SCHEDULE_ONCHIP || pk_onchip_plan(h, why)) cand.push_back({PARADMM_SCHEDULE_ONCHIP, 0, 0, 0});
-        else cudaGetLastError();
+        // the cluster-resident schedule only when the handle asked for it: on
+        // batches it runs fewer instances at once and loses to the tiled one
+        if (P.schedule == PARADMM_SCHEDULE_ONCHIP) cand.push_back({PARADMM_SCHEDULE_ONCHIP, 0, 0, 0});
     }
     const int saved_schedule = P.schedule, saved_cluster = P.cluster, saved_coop = P.coop_min_n;
     const int saved_fallback = P.fallback_after;
@@ -2358,6 +2359,143 @@ extern "C" int paradmm_gpu_shard_finish(paradmm_gpu *h, void *stream, paradmm_st
         stats->total_radius = NAN;
     }
     return rc;
+}
+
+extern "C" int paradmm_gpu_shard_fused_buffers(paradmm_gpu *h, void **exchange, void **flags)
+{
+    ok_status();
+    PkHost *Pp;
+    int rc = shard_handle(h, &Pp);
+    if (rc) return rc;
+    PkHost &P = *Pp;
+    if (P.shard_n > PK_XCH_MAX) return pdm_set_error(PARADMM_EINVAL, "the fused exchange takes at most %d ranks", PK_XCH_MAX);
+    DevGuard guard(h->device);
+    if (!P.d_fx_exch) {
+        const size_t nx = 2ull * (size_t)P.shard_n * (size_t)P.inst[0].N * sizeof(double4);
+        if ((rc = dalloc(h, (void **)&P.d_fx_exch, nx))) return rc;
+        if ((rc = dalloc(h, (void **)&P.d_fx_flags, sizeof(unsigned long long) * P.shard_n))) return rc;
+        PDM_CUDA(cudaMemset(P.d_fx_exch, 0, nx));
+        PDM_CUDA(cudaMemset(P.d_fx_flags, 0, sizeof(unsigned long long) * P.shard_n));
+    }
+    if (exchange) *exchange = P.d_fx_exch;
+    if (flags) *flags = P.d_fx_flags;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_shard_run_fused(paradmm_gpu *const *hs, int nlocal, void *const *exchanges,
+                                           void *const *flags, int wait_ms, void *stream)
+{
+    ok_status();
+    if (!hs || nlocal < 1 || nlocal > PK_XCH_MAX) return pdm_set_error(PARADMM_EINVAL, "nlocal must be 1 .. %d", PK_XCH_MAX);
+    if (!exchanges || !flags) return pdm_set_error(PARADMM_EINVAL, "exchanges and flags are required");
+    PkHost *L[PK_XCH_MAX];
+    for (int i = 0; i < nlocal; ++i) {
+        int rc = shard_handle(hs[i], &L[i]);
+        if (rc) return rc;
+    }
+    PkHost &P0 = *L[0];
+    const int R = P0.shard_n, rank0 = P0.shard_rank;
+    if (R > PK_XCH_MAX) return pdm_set_error(PARADMM_EINVAL, "the fused exchange takes at most %d ranks", PK_XCH_MAX);
+    if (rank0 + nlocal > R) return pdm_set_error(PARADMM_EINVAL, "more local ranks than ranks");
+    for (int i = 0; i < nlocal; ++i) {
+        const PkHost &P = *L[i];
+        if (hs[i]->device != hs[0]->device) return pdm_set_error(PARADMM_EINVAL, "the local ranks must share one device");
+        if (P.shard_n != R || P.shard_rank != rank0 + i)
+            return pdm_set_error(PARADMM_EINVAL, "local ranks must be consecutive shards of one split");
+        if (P.V != P0.V || P.stream_hint != P0.stream_hint || P.inst[0].N != P0.inst[0].N)
+            return pdm_set_error(PARADMM_EINVAL, "local ranks differ in instance or tile side");
+        if (!P.shard_running || P.shard_phase != 0 || P.shard_k != P.shard_it0)
+            return pdm_set_error(PARADMM_EINVAL, "each rank needs a fresh run (paradmm_gpu_shard_start) to fuse");
+        if (P.shard_it0 != P0.shard_it0 || P.shard_stop != P0.shard_stop || P.shard_tol != P0.shard_tol ||
+            P.shard_check_every != P0.shard_check_every || P.fx_epoch != P0.fx_epoch)
+            return pdm_set_error(PARADMM_EINVAL, "local ranks are not at the same point of the same run");
+    }
+    PkXch X{};
+    X.nranks = R;
+    X.rank0 = rank0;
+    X.nlocal = nlocal;
+    X.epoch = P0.fx_epoch + 1;
+    for (int q = 0; q < R; ++q) {
+        if (!exchanges[q] || ((uintptr_t)exchanges[q] & 15u) || !flags[q] || ((uintptr_t)flags[q] & 7u))
+            return pdm_set_error(PARADMM_EINVAL, "rank %d: exchange (16-byte) or flag (8-byte) buffer missing or misaligned", q);
+        X.exch[q] = (double4 *)exchanges[q];
+        X.flag[q] = (unsigned long long *)flags[q];
+    }
+    DevGuard guard(hs[0]->device);
+    int bps = 0;
+    cudaError_t e = pk_shard_fused_blocks(P0.V, P0.stream_hint, &bps);
+    if (e != cudaSuccess || bps < 1) return pdm_cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidConfiguration, "fused shard occupancy", __FILE__, __LINE__);
+    X.blocks = bps * hs[0]->num_sms / nlocal;
+    if (X.blocks < 1) return pdm_set_error(PARADMM_EINVAL, "too many local ranks for one device");
+    PkDev devs[PK_XCH_MAX];
+    for (int i = 0; i < nlocal; ++i) {
+        devs[i] = L[i]->D;
+        X.row_lo[i] = L[i]->row_lo;
+        X.row_hi[i] = L[i]->row_hi;
+    }
+    int rc;
+    if (!P0.d_fx_devs && (rc = dalloc(hs[0], (void **)&P0.d_fx_devs, sizeof(PkDev) * PK_XCH_MAX))) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : hs[0]->stream;
+    PDM_CUDA(cudaMemcpyAsync(P0.d_fx_devs, devs, sizeof(PkDev) * nlocal, cudaMemcpyHostToDevice, s));
+    const unsigned long long lim = wait_ms > 0 ? (unsigned long long)wait_ms * 1000000ull : 0ull;
+    for (int i = 0; i < nlocal; ++i)
+        PDM_CUDA(cudaMemcpyAsync((char *)hs[i]->ctl + offsetof(DevCtl, timeout_ns), &lim, sizeof lim, cudaMemcpyHostToDevice, s));
+    PkRun Rr{};
+    Rr.it0 = P0.shard_k;
+    Rr.n_iter = (int)std::min<long long>(P0.shard_stop - P0.shard_k, INT_MAX);
+    Rr.dynamic = 1;
+    Rr.tol = P0.shard_tol;
+    Rr.check_every = P0.shard_check_every;
+    Rr.bal_period = P0.bal_period;
+    Rr.bal_mu = P0.bal_mu;
+    Rr.bal_lmin = P0.bal_lmin;
+    Rr.bal_lmax = P0.bal_lmax;
+    Rr.bal_any = pk_bal_any(P0);
+    e = pk_launch_shard_fused(P0.V, P0.stream_hint, P0.d_fx_devs, Rr, X, s);
+    if (e != cudaSuccess) return pdm_cuda_fail(e, "fused shard launch", __FILE__, __LINE__);
+    PDM_CUDA(cudaStreamSynchronize(s));
+    rc = PARADMM_OK;
+    for (int i = 0; i < nlocal; ++i) {
+        PkHost &P = *L[i];
+        DevCtl c{};
+        PDM_CUDA(cudaMemcpy(&c, hs[i]->ctl, sizeof c, cudaMemcpyDeviceToHost));
+        ++hs[i]->launches;
+        P.fx_epoch = X.epoch;
+        P.shard_k = P.shard_it0 + (long long)c.pad[0];
+        if (c.err != DEV_OK && rc == PARADMM_OK)
+            rc = pdm_set_error(PARADMM_ETIMEOUT, "fused shard kernel, rank %d: a device-side wait ran out (%s)",
+                               P.shard_rank, pdm_dev_err_name(c.err));
+    }
+    return rc;
+}
+
+extern "C" int paradmm_gpu_ipc_export(const void *dev_ptr, void *handle)
+{
+    ok_status();
+    if (!dev_ptr || !handle) return pdm_set_error(PARADMM_EINVAL, "dev_ptr and handle are required");
+    cudaIpcMemHandle_t hd;
+    PDM_CUDA(cudaIpcGetMemHandle(&hd, const_cast<void *>(dev_ptr)));
+    memcpy(handle, &hd, sizeof hd);
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_ipc_import(int device, const void *handle, void **dev_ptr)
+{
+    ok_status();
+    if (!handle || !dev_ptr) return pdm_set_error(PARADMM_EINVAL, "handle and dev_ptr are required");
+    DevGuard guard(device);
+    cudaIpcMemHandle_t hd;
+    memcpy(&hd, handle, sizeof hd);
+    PDM_CUDA(cudaIpcOpenMemHandle(dev_ptr, hd, cudaIpcMemLazyEnablePeerAccess));
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_ipc_close(int device, void *dev_ptr)
+{
+    ok_status();
+    DevGuard guard(device);
+    PDM_CUDA(cudaIpcCloseMemHandle(dev_ptr));
+    return PARADMM_OK;
 }
 
 extern "C" void paradmm_gpu_destroy(paradmm_gpu *h)

@@ -102,6 +102,11 @@ struct PkHost {
     int shard_n = 0, shard_rank = 0, row_lo = 0, row_hi = -1;
     int shard_running = 0, shard_phase = 0;  // a run is armed; 1 = the exchange of sweep shard_k is pending
     long long shard_it0 = 0, shard_k = 0, shard_stop = 0;  // first sweep of the run, next sweep, end of the run
+    // fused exchange (paradmm_gpu_shard_run_fused)
+    double4 *d_fx_exch = nullptr;              // [2][shard_n][N] partial sums, by sweep parity and rank
+    unsigned long long *d_fx_flags = nullptr;  // [shard_n] each rank's (epoch, sweep) flag
+    PkDev *d_fx_devs = nullptr;                // [PK_XCH_MAX] the local ranks' device views for one launch
+    unsigned long long fx_epoch = 0;           // fused launches run so far (the flag epoch)
     double shard_tol = -1.0;
     int shard_check_every = 1;
     unsigned *d_done = nullptr;      // CTAs of the running consensus launch that finished

@@ -26,6 +26,23 @@ cudaError_t pk_launch_shard_begin(int V, bool stream_hint, const PkDev &D, const
 cudaError_t pk_launch_shard_end(int V, const PkDev &D, const PkRun &R, long long k, int nb, const double4 *exch,
                                 unsigned *done, cudaStream_t s);
 
+// The sharded instance's fused sweep loop (pk_shard_fused): ranks
+// [rank0, rank0 + nlocal) of `nranks` run in one cooperative launch on this
+// device, `blocks` CTAs each; every rank's exchange buffer and flag array
+// is given as this device sees it (its own memory, or a peer GPU's mapped
+// into this process).
+#define PK_XCH_MAX 8
+struct PkXch {
+    int nranks, rank0, nlocal, blocks;
+    unsigned long long epoch;                    // flag epoch of this launch (the same on every rank)
+    double4 *exch[PK_XCH_MAX];                   // rank q's exchange buffer: [2][nranks][N] double4
+    unsigned long long *flag[PK_XCH_MAX];        // rank q's flags: [nranks]
+    int row_lo[PK_XCH_MAX], row_hi[PK_XCH_MAX];  // block rows of the local ranks
+};
+cudaError_t pk_shard_fused_blocks(int V, bool stream_hint, int *blocks_per_sm);
+cudaError_t pk_launch_shard_fused(int V, bool stream_hint, const PkDev *devs, const PkRun &R, const PkXch &X,
+                                  cudaStream_t s);
+
 // Cluster-resident solver (onchip_kernels.cu).  Instances of size class c
 // need a group of 2^c CTAs (c = 0 .. OC_CLASSES - 1).
 #define OC_MAX_WALLS 4    // walls per circle the solver holds on chip

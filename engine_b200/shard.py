@@ -66,6 +66,12 @@ class Shard(Handle):
         check(self.lib.paradmm_gpu_shard_poll(self.ptr, C.c_void_p(stream or None), C.byref(a)))
         return bool(a.value)
 
+    def fused_buffers(self) -> tuple[int, int]:
+        """(exchange, flags) device pointers of this rank for the fused run."""
+        ex, fl = C.c_void_p(), C.c_void_p()
+        check(self.lib.paradmm_gpu_shard_fused_buffers(self.ptr, C.byref(ex), C.byref(fl)))
+        return ex.value, fl.value
+
     def finish(self, stream: int = 0) -> dict:
         s = Stats()
         rc = self.lib.paradmm_gpu_shard_finish(self.ptr, C.c_void_p(stream or None), C.byref(s))
@@ -120,6 +126,69 @@ def solve(desc: dict, maxiter: int, tol: float, group=None, poll_every: int = 64
             dist.all_reduce(t, group=group)
 
     return shard, run_sharded(shard, exchange, allreduce, maxiter, tol, poll_every)
+
+
+def run_fused(shards, exchanges, flags, wait_ms: int = 0, stream: int = 0) -> None:
+    """paradmm_gpu_shard_run_fused: the armed runs of `shards` (consecutive
+    ranks on one device) in one persistent launch with the exchange fused in.
+    exchanges[q] / flags[q]: rank q's buffers as this device addresses them,
+    for every rank q of the split."""
+    lib = load()
+    n = len(shards)
+    hs = (C.c_void_p * n)(*[s.ptr for s in shards])
+    R = len(exchanges)
+    ex = (C.c_void_p * R)(*exchanges)
+    fl = (C.c_void_p * R)(*flags)
+    check(lib.paradmm_gpu_shard_run_fused(hs, n, ex, fl, int(wait_ms), C.c_void_p(stream or None)))
+
+
+def solve_fused(desc: dict, maxiter: int, tol: float, group=None, wait_ms: int = 0, **kw) -> tuple[Shard, dict]:
+    """One instance over the ranks of `group` (torch.distributed, one rank per
+    GPU) in one persistent launch per GPU: the ranks' exchange buffers and
+    flags are shared through CUDA IPC, each rank's kernel stores its partial
+    sums into every peer's buffer over NVLink and waits on their flags; the
+    only host collectives are the handle exchange before the run and a
+    barrier after it."""
+    import torch
+    import torch.distributed as dist
+
+    lib = load()
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    dev = torch.cuda.current_device()
+    shard = Shard(desc, rank, world, device=dev, **kw)
+    ex, fl = shard.fused_buffers()
+    mine = [bytes(64), bytes(64)]
+    for j, ptr in enumerate((ex, fl)):
+        buf = C.create_string_buffer(64)
+        check(lib.paradmm_gpu_ipc_export(C.c_void_p(ptr), buf))
+        mine[j] = buf.raw
+    every = [None] * world
+    if world > 1:
+        dist.all_gather_object(every, (rank, mine[0], mine[1]), group=group)
+    else:
+        every = [(rank, mine[0], mine[1])]
+    exchanges, flags, opened = [0] * world, [0] * world, []
+    try:
+        for q, hx, hf in every:
+            if q == rank:
+                exchanges[q], flags[q] = ex, fl
+                continue
+            for j, hnd in enumerate((hx, hf)):
+                p = C.c_void_p()
+                check(lib.paradmm_gpu_ipc_import(dev, C.create_string_buffer(hnd, 64), C.byref(p)))
+                opened.append(p.value)
+                (exchanges if j == 0 else flags)[q] = p.value
+        shard.start(maxiter, tol)
+        stream = torch.cuda.current_stream().cuda_stream
+        run_fused([shard], exchanges, flags, wait_ms, stream)
+        stats = shard.finish(stream)
+    finally:
+        if world > 1:
+            dist.barrier(group=group)  # no rank still writes into a buffer about to be unmapped
+        for p in opened:
+            lib.paradmm_gpu_ipc_close(dev, C.c_void_p(p))
+    return shard, stats
 
 
 # ------------------------------------------------------- batches over ranks

@@ -373,6 +373,40 @@ int paradmm_gpu_shard_end(paradmm_gpu *h, const void *exchange, void *stream);
 int paradmm_gpu_shard_poll(paradmm_gpu *h, void *stream, int *active);
 int paradmm_gpu_shard_finish(paradmm_gpu *h, void *stream, paradmm_stats *stats);
 
+/* The whole armed run in ONE persistent launch per device, with the exchange
+ * fused into it: each rank writes its partial sums straight into slot r of
+ * every rank's exchange buffer (peer stores over NVLink), raises its flag in
+ * every rank's flag array, waits (bounded) for all ranks' flags of the sweep
+ * and sums the slots in rank order, so every rank holds the same Z and takes
+ * the same stop decision; no host round trip, no collective library call.
+ *
+ * paradmm_gpu_shard_fused_buffers allocates (once) and returns this rank's
+ * exchange buffer (2 x nranks x n_circles x 32 bytes) and flag array
+ * (nranks x 8 bytes) on its device; a multi-process caller shares them
+ * between processes (CUDA IPC) and maps the peers' into each process.
+ *
+ * paradmm_gpu_shard_run_fused(hs, nlocal, exchanges, flags, wait_ms, stream)
+ * runs ranks hs[0 .. nlocal) -- consecutive ranks of one split, on one
+ * device, each armed by paradmm_gpu_shard_start and not yet stepped -- in
+ * one cooperative launch; exchanges[q] and flags[q] are rank q's buffers as
+ * this device addresses them, for every q < nranks.  One process per GPU
+ * passes nlocal = 1; every rank must launch (all ranks' kernels run at the
+ * same time, one per GPU), or, on one device, all ranks go in one call.  A
+ * flag that does not arrive within wait_ms (0: 4 s) ends the launch with
+ * PARADMM_ETIMEOUT.  It returns when the run has ended (stop test or
+ * maxiter); paradmm_gpu_shard_finish then reads the statistics.  At most 8
+ * ranks. */
+int paradmm_gpu_shard_fused_buffers(paradmm_gpu *h, void **exchange, void **flags);
+int paradmm_gpu_shard_run_fused(paradmm_gpu *const *hs, int nlocal, void *const *exchanges, void *const *flags,
+                                int wait_ms, void *stream);
+
+/* Process-to-process sharing of those buffers (CUDA IPC; the handle is 64
+ * bytes): export a device allocation's base pointer, import it on `device`
+ * (peer access enabled on first use), close an imported pointer. */
+int paradmm_gpu_ipc_export(const void *dev_ptr, void *handle /* 64 bytes */);
+int paradmm_gpu_ipc_import(int device, const void *handle, void **dev_ptr);
+int paradmm_gpu_ipc_close(int device, void *dev_ptr);
+
 /* ---- allocation-free packing sweeps ----
  *
  * Some callers cannot allocate device memory while they run: services that
