@@ -125,13 +125,18 @@ class Clocks:
 
     def _poll(self):
         nv = self.nv
+        try:
+            mx = [nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM) for h in self.h]  # fixed per device
+        except Exception as ex:
+            self.err = str(ex)[:80]
+            self.run = False
+            return
         while self.run:
-            for h in self.h:
+            for h, m in zip(self.h, mx):
                 try:
                     sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                    mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
                     rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                    self.rows.append((time.perf_counter(), sm, mx, rs))
+                    self.rows.append((time.perf_counter(), sm, m, rs))
                     time.sleep(0.0002)
                 except Exception as ex:
                     self.err = str(ex)[:80]
