@@ -150,6 +150,8 @@ _SIGS = {
     "paradmm_gpu_launches": (C.c_int64, [C.c_void_p]),
     "paradmm_gpu_instance_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "paradmm_gpu_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "paradmm_gpu_set_tail_handoff": (C.c_int, [C.c_void_p, C.c_int]),
+    "paradmm_gpu_tail_handoffs": (C.c_int, [C.c_void_p]),
     "paradmm_gpu_set_fallback": (C.c_int, [C.c_void_p, C.c_int64]),
     "paradmm_gpu_set_rho_balance": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
     "paradmm_gpu_rho_scale": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
@@ -485,6 +487,14 @@ class Handle:
 
     def launches(self) -> int:
         return self.lib.paradmm_gpu_launches(self.ptr)
+
+    def set_tail_handoff(self, instances: int) -> None:
+        """paradmm_gpu_set_tail_handoff: the last `instances` unfinished
+        instances of a per-instance solve finish on the grid schedule."""
+        check(self.lib.paradmm_gpu_set_tail_handoff(self.ptr, int(instances)))
+
+    def tail_handoffs(self) -> int:
+        return self.lib.paradmm_gpu_tail_handoffs(self.ptr)
 
     def set_profiling(self, on: bool) -> None:
         check(self.lib.paradmm_gpu_set_profiling(self.ptr, 1 if on else 0))

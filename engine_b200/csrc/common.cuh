@@ -28,7 +28,7 @@ static inline const char *pdm_dev_err_name(int e)
 // launch.
 struct DevCtl {
     unsigned int bar_count;   // grid-barrier arrivals in this launch
-    unsigned int bar_pad;
+    unsigned int n_done;      // per-instance schedule: instances whose solve in this launch has ended
     int err;                  // DEV_* error, first writer wins
     int n_active;             // instances still iterating
     unsigned int item_ctr[2]; // dynamic work counters, one per iteration parity

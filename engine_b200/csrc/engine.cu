@@ -592,12 +592,15 @@ static int pk_finalize_build(paradmm_gpu *h)
     PkDev &D = P.D;
     D.n_inst = P.n_inst;
     D.n_items = P.n_items;
+    D.n_claim = P.n_items;
     D.n_circ = P.n_circ;
     D.n_fin = (int)fin.size();
+    D.n_finl = D.n_fin;
     int rc;
     if ((rc = dput(h, (PkInst **)&D.inst, P.inst))) return rc;
     if ((rc = dput(h, (int4 **)&D.items, P.items))) return rc;
     if ((rc = dput(h, (int **)&D.claim, claim))) return rc;
+    P.claim_order = claim;
     if ((rc = dput(h, (PkCircle **)&D.circ, P.circ))) return rc;
     const long long tile_bytes = pk_tile_floats(P.BW) * 4LL;
     if ((rc = dalloc(h, (void **)&D.tiles, (size_t)(P.n_tiles * tile_bytes)))) return rc;
@@ -614,6 +617,7 @@ static int pk_finalize_build(paradmm_gpu *h)
     }
     if ((rc = dalloc(h, (void **)&D.local_part, sizeof(double4) * (size_t)P.n_circ))) return rc;
     if ((rc = dput(h, (int2 **)&D.fin_items, fin))) return rc;
+    P.fin_list = fin;
     if ((rc = dalloc(h, (void **)&D.blk_primal, sizeof(double) * 4 * (size_t)D.n_fin))) return rc;
     if ((rc = dalloc(h, (void **)&D.blk_dual, sizeof(double) * 4 * (size_t)D.n_fin))) return rc;
     PDM_CUDA(cudaMemset(D.blk_primal, 0, sizeof(double) * 4 * (size_t)D.n_fin));
@@ -1051,6 +1055,9 @@ static void pk_drop_graph(PkHost &P)
     P.graph_exec = nullptr;
 }
 
+static int pk_run_grid(paradmm_gpu *h, long long n, double tol, int check_every, double *ms,
+                       const std::vector<char> *skip, const std::vector<long long> *budget, const PkDev *Dv);
+
 static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_every, double *ms)
 {
     PkHost &P = *h->pk;
@@ -1070,6 +1077,7 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
         s.pad = 0;
         s.t_begin_ns = s.t_end_ns = 0;
         s.bal_base = -P.age[i];  // sweep 0 of this call produces the iterate of age age[i] + 1
+        s.yield_at = 0;
     }
     PkRun R{};
     R.it0 = 0;
@@ -1084,8 +1092,12 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
     R.bal_lmin = P.bal_lmin;
     R.bal_lmax = P.bal_lmax;
     R.bal_any = pk_bal_any(P);
+    // the tail hand-off needs the grid-wide schedule to take over; a fallback
+    // budget (restart inside the launch) exists on the per-instance schedule only
+    R.yield_below = (P.schedule == PARADMM_SCHEDULE_INSTANCE && R.fallback_after == 0) ? P.tail_yield : 0;
     PkGraphKey key;
     memset(&key, 0, sizeof key);
+    key.yield_below = R.yield_below;
     key.bal_period = R.bal_period;
     key.bal_mu = R.bal_mu;
     key.bal_lmin = R.bal_lmin;
@@ -1148,18 +1160,64 @@ static int pk_run_instances(paradmm_gpu *h, long long n, double tol, int check_e
         if (st.nonfinite) rc = pdm_set_error(PARADMM_ENONFINITE, "instance %d: residual became NaN/Inf", i);
     }
     P.it_next += n;
+    if (rc != PARADMM_OK || R.yield_below <= 0) return rc;
+    // tail hand-off: the instances that stopped for it continue on the
+    // grid-wide schedule for the rest of their budget of n sweeps
+    std::vector<char> skip(P.n_inst, 1);
+    std::vector<long long> budget(P.n_inst, 0);
+    int nyield = 0;
+    for (int i = 0; i < P.n_inst; ++i) {
+        const PkStatus &st = P.status[i];
+        if (st.yield_at > 0 && st.last_iter == st.yield_at && !st.converged && !st.nonfinite &&
+            P.iters_last_call[i] < n) {
+            skip[i] = 0;
+            budget[i] = n - P.iters_last_call[i];
+            ++nyield;
+        }
+    }
+    P.yielded_last_call = nyield;
+    if (nyield == 0) return rc;
+    // the grid-wide launches claim only these instances' work items and run
+    // only their consensus items
+    std::vector<int> claim, fin;
+    for (int q : P.claim_order)
+        if (!skip[P.items[q].x]) claim.push_back(q);
+    for (const int2 &f : P.fin_list)
+        if (!skip[f.x]) fin.push_back(f.x), fin.push_back(f.y);
+    if (!P.d_claim_tail) {
+        if ((rc = dalloc(h, (void **)&P.d_claim_tail, sizeof(int) * (size_t)P.n_items))) return rc;
+        if ((rc = dalloc(h, (void **)&P.d_fin_tail, sizeof(int2) * P.fin_list.size()))) return rc;
+    }
+    PDM_CUDA(cudaMemcpyAsync(P.d_claim_tail, claim.data(), sizeof(int) * claim.size(), cudaMemcpyHostToDevice, h->stream));
+    PDM_CUDA(cudaMemcpyAsync(P.d_fin_tail, fin.data(), sizeof(int) * fin.size(), cudaMemcpyHostToDevice, h->stream));
+    PkDev Dv = P.D;
+    Dv.claim = P.d_claim_tail;
+    Dv.n_claim = (int)claim.size();
+    Dv.fin_items = P.d_fin_tail;
+    Dv.n_finl = (int)(fin.size() / 2);
+    double ms2 = 0;
+    rc = pk_run_grid(h, n, tol, check_every, &ms2, &skip, &budget, &Dv);
+    if (ms) *ms += ms2;
     return rc;
 }
 
-static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, double *ms)
+// Grid-wide schedule: up to n sweeps of every instance not in `skip`, and
+// at most budget[i] sweeps of instance i when `budget` is given (a finite
+// last_iter per launch); iteration counts add to P.iters_last_call.
+static int pk_run_grid(paradmm_gpu *h, long long n, double tol, int check_every, double *ms,
+                       const std::vector<char> *skip, const std::vector<long long> *budget, const PkDev *Dv)
 {
     PkHost &P = *h->pk;
-    std::fill(P.iters_last_call.begin(), P.iters_last_call.end(), 0LL);
-    if (P.schedule == PARADMM_SCHEDULE_INSTANCE || P.schedule == PARADMM_SCHEDULE_ONCHIP)
-        return pk_run_instances(h, n, tol, check_every, ms);
     std::vector<char> done(P.n_inst, 0);
+    std::vector<long long> ran_here(P.n_inst, 0);
+    if (skip) done = *skip;
     double total_ms = 0;
     long long left = n;
+    if (budget) {
+        left = 0;
+        for (int i = 0; i < P.n_inst; ++i)
+            if (!done[i]) left = std::max(left, std::min(n, (*budget)[i]));
+    }
     int rc = PARADMM_OK;
     while (left > 0) {
         const int chunk = (int)std::min<long long>(left, PK_SWEEPS_PER_LAUNCH);
@@ -1169,7 +1227,9 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
         for (int i = 0; i < P.n_inst; ++i) {
             PkStatus &s = st[i];
             s = P.status[i];
+            if (!done[i] && budget && (*budget)[i] - ran_here[i] <= 0) done[i] = 1;
             s.last_iter = done[i] ? it0 - 1 : LLONG_MAX;
+            if (!done[i] && budget) s.last_iter = it0 + (*budget)[i] - ran_here[i] - 1;
             s.check_from = it0 + 2;
             s.converged = 0;
             s.nonfinite = 0;
@@ -1199,7 +1259,7 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
         R.bal_lmax = P.bal_lmax;
     R.bal_any = pk_bal_any(P);
         PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
-        cudaError_t e = pk_launch_persistent(P.V, P.stream_hint, P.D, R, P.grid, h->stream);
+        cudaError_t e = pk_launch_persistent(P.V, P.stream_hint, Dv ? *Dv : P.D, R, P.grid, h->stream);
         if (e != cudaSuccess) return pdm_cuda_fail(e, "packing persistent launch", __FILE__, __LINE__);
         ++h->launches;
         PDM_CUDA(cudaEventRecord(h->ev1, h->stream));
@@ -1218,7 +1278,7 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
             if (done[i]) continue;
             const long long last = std::min(st[i].last_iter, it0 + sweeps - 1);
             const long long ran = last - it0 + 1;
-            if (ran > 0) P.iters_last_call[i] += ran;
+            if (ran > 0) { P.iters_last_call[i] += ran; ran_here[i] += ran; }
             if (ran > 0) { P.age[i] += ran; P.last_swept[i] = last; }
             P.nmode[i] = pk_pending_mode(st[i], last);
             P.status[i] = st[i];
@@ -1231,6 +1291,16 @@ static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, doub
     }
     if (ms) *ms = total_ms;
     return rc;
+}
+
+static int pk_run(paradmm_gpu *h, long long n, double tol, int check_every, double *ms)
+{
+    PkHost &P = *h->pk;
+    std::fill(P.iters_last_call.begin(), P.iters_last_call.end(), 0LL);
+    P.yielded_last_call = 0;
+    if (P.schedule == PARADMM_SCHEDULE_INSTANCE || P.schedule == PARADMM_SCHEDULE_ONCHIP)
+        return pk_run_instances(h, n, tol, check_every, ms);
+    return pk_run_grid(h, n, tol, check_every, ms, nullptr, nullptr, nullptr);
 }
 
 // ===========================================================================
@@ -1685,6 +1755,21 @@ extern "C" int paradmm_gpu_instance_times(const paradmm_gpu *h, double *begin_ms
         end_ms[i] = P.status[i].t_end_ns ? (double)(P.status[i].t_end_ns - t0) * 1e-6 : NAN;
     }
     return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_set_tail_handoff(paradmm_gpu *h, int instances)
+{
+    ok_status();
+    if (!h || !h->pk) return pdm_set_error(PARADMM_EINVAL, "the tail hand-off needs a packing handle");
+    if (instances < 0) return pdm_set_error(PARADMM_EINVAL, "instances < 0");
+    if (h->pk->shard_n > 0) return pdm_set_error(PARADMM_EINVAL, "a shard of an instance has no per-instance schedule");
+    h->pk->tail_yield = instances;
+    return PARADMM_OK;
+}
+
+extern "C" int paradmm_gpu_tail_handoffs(const paradmm_gpu *h)
+{
+    return h && h->pk ? h->pk->yielded_last_call : 0;
 }
 
 extern "C" int paradmm_gpu_set_profiling(paradmm_gpu *h, int on)

@@ -35,7 +35,7 @@ struct PkGraphKey {
     int check_every, fallback_after, prof, cluster, n_coop, inst_grid, n_early;
     int bal_period, bal_lmin, bal_lmax;
     double bal_mu;
-    int schedule, bal_any;
+    int schedule, bal_any, yield_below;
 };
 
 struct PkHost {
@@ -84,6 +84,12 @@ struct PkHost {
     int *d_order = nullptr;          // the same on the device
     int prof = 0;                    // per-phase timing requested
     int fallback_after = 0;          // per-instance schedule: restart from the plain start after this many sweeps
+    int tail_yield = 0;              // per-instance schedule: hand the last this-many instances to the grid schedule
+    int yielded_last_call = 0;       // instances the last solve call handed over
+    std::vector<int> claim_order;    // the grid schedule's item claim order (host copy of D.claim)
+    std::vector<int2> fin_list;      // consensus items (host copy of D.fin_items)
+    int *d_claim_tail = nullptr;     // claim order / consensus items of the handed-over instances
+    int2 *d_fin_tail = nullptr;
     // per-instance schedule: the solve call's launch sequence as a CUDA graph
     int use_graphs = 1;
     cudaGraphExec_t graph_exec = nullptr;

@@ -214,6 +214,7 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     D.circ = (const PkCircle *)(base + NaLayout::circ);
     D.n_inst = 1;
     D.n_items = n_items;
+    D.n_claim = n_items;
     D.n_circ = N;
     D.row_part = (double4 *)(base + NaLayout::row_part);
     D.col_part = (double4 *)(base + NaLayout::col_part);
@@ -221,6 +222,7 @@ extern "C" int paradmm_gpu_packing_iterate_noalloc(const paradmm_packing_desc *d
     D.local_part = (double4 *)(base + NaLayout::local_part);
     D.fin_items = (const int2 *)(base + NaLayout::fin_items);
     D.n_fin = s_inst.nb;
+    D.n_finl = s_inst.nb;
     D.blk_primal = (double *)(base + NaLayout::blk_primal);
     D.blk_dual = (double *)(base + NaLayout::blk_dual);
     D.status = (PkStatus *)(base + NaLayout::status);

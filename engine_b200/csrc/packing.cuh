@@ -119,7 +119,7 @@ struct PkStatus {
     int bal_log2_new;        // ... from bal_pass_age on
     double sd_last;          // per-instance schedule: dual-residual sum of the last consensus run
     int sd_valid;            // sd_last belongs to the state the next call continues
-    int pad3;
+    int yield_at;            // per-instance schedule: sweep at which the instance stops for the grid-wide schedule (0: none)
 };
 
 // Device pointers of a packing handle (passed by value to kernels).
@@ -127,8 +127,8 @@ struct PkDev {
     const PkInst *inst;
     const int4 *items;
     const PkCircle *circ;
-    const int *claim;        // [n_items] order in which blocks claim items (largest first)
-    int n_inst, n_items, n_circ, pad;
+    const int *claim;        // [n_claim] order in which blocks claim items (largest first)
+    int n_inst, n_items, n_circ, n_claim;  // n_claim: items in `claim` (n_items, or a subset's)
     float *tiles;            // pair state
     double4 *row_part;       // [tile][BW] sums of M over the row circle's pair edges; w: their primal-residual sum
     double4 *col_part;       // [tile][BW] same for the column circle
@@ -137,8 +137,8 @@ struct PkDev {
     float4 *Zp;              // [circle] Z of the previous sweep (FP32: the values the pass used)
     float *aux;              // N of the pair edges for PK_MODE_N (tile layout; graph handles only)
     double4 *local_part;     // [circle] rho-weighted wall + radius contributions; w: their primal-residual sum
-    const int2 *fin_items;   // [n_fin] consensus items (instance, circle block)
-    int n_fin, pad2;
+    const int2 *fin_items;   // [n_finl] consensus items (instance, circle block) the grid schedule runs
+    int n_fin, n_finl;       // n_fin: all consensus items (the stride of blk_*); n_finl: items in fin_items
     double *blk_primal;      // [4][n_fin] per consensus item, by sweep index mod 4
     double *blk_dual;        // [4][n_fin]
     PkStatus *status;        // [n_inst]
@@ -167,7 +167,8 @@ struct PkRun {
     double bal_mu;    // ... double the penalties when r > mu s, halve them when s > mu r
     int bal_lmin, bal_lmax;  // ... within scales 2^bal_lmin .. 2^bal_lmax
     int bal_any;      // balancing on, or some instance's penalties not at scale 1: passes read the scale
-    int pad3;
+    int yield_below;  // per-instance schedule: once every instance has started and at most this many are
+                      // unfinished, they stop (yielded) for the grid-wide schedule to finish (0: never)
 };
 
 // Residual balancing of the penalties (no reference counterpart: the

@@ -142,6 +142,14 @@ class Batch:
     def set_rho_balance(self, period: int, mu: float = 10.0, log2_min: int = -1, log2_max: int = 4) -> None:
         check(self.lib.paradmm_gpu_set_rho_balance(self.h, int(period), float(mu), int(log2_min), int(log2_max)))
 
+    def set_tail_handoff(self, instances: int) -> None:
+        """The last `instances` unfinished instances of a solve finish together
+        on the grid-wide schedule (paradmm_gpu_set_tail_handoff)."""
+        check(self.lib.paradmm_gpu_set_tail_handoff(self.h, int(instances)))
+
+    def tail_handoffs(self) -> int:
+        return self.lib.paradmm_gpu_tail_handoffs(self.h)
+
     def fallbacks(self) -> np.ndarray:
         out = np.zeros(len(self.instances), dtype=np.int32)
         check(self.lib.paradmm_gpu_instance_fallbacks(self.h, out.ctypes.data_as(C.POINTER(C.c_int))))

@@ -318,6 +318,17 @@ int64_t paradmm_gpu_launches(const paradmm_gpu *h);
  * block/cluster barrier after it, the consensus, and the barrier plus stop
  * test); paradmm_gpu_phase_times returns those four means (microseconds)
  * for the last solve/iterate call. */
+/* Tail hand-off of the per-instance schedule: once every instance of a
+ * solve call has started and at most `instances` are unfinished, those stop
+ * at a sweep boundary and finish together on the grid-wide schedule (one
+ * pass over all their tiles by every CTA per sweep, instead of one pass per
+ * instance by its own few CTAs); each keeps its own budget of maxiter sweeps
+ * and its own stop test.  0 (default): off.  Not combined with a fallback
+ * budget (paradmm_gpu_set_fallback).  paradmm_gpu_tail_handoffs: instances
+ * the last solve call handed over. */
+int paradmm_gpu_set_tail_handoff(paradmm_gpu *h, int instances);
+int paradmm_gpu_tail_handoffs(const paradmm_gpu *h);
+
 int paradmm_gpu_set_profiling(paradmm_gpu *h, int on);
 int paradmm_gpu_phase_times(const paradmm_gpu *h, double out[4]);
 
