@@ -58,9 +58,14 @@ def test_handed_over_instances_stop_on_their_own_residual(cluster, coop):
         # the grid schedule tests iterate k - 2 at sweep k (the per-instance
         # one k - 1): a handed-over instance may take one sweep more
         assert 0 <= b["iterations"] - a["iterations"] <= 2 or not a["converged"], (a["iterations"], b["iterations"])
+    # stopped at r + s <= 1e-5, up to two sweeps apart: the packings agree to
+    # the size of a sweep's step there
+    for a, b, x, y in zip(st0, st1, c0, c1):
+        if a["converged"]:
+            assert np.abs(x - y).max() <= 1e-3
     tot0 = sum(c[:, 2].sum() for c in c0)
     tot1 = sum(c[:, 2].sum() for c in c1)
-    assert abs(tot1 - tot0) <= 1e-6 * tot0
+    assert abs(tot1 - tot0) <= 1e-4 * tot0
 
 
 def test_no_handoff_with_a_fallback_budget():
