@@ -68,11 +68,15 @@ def test_handed_over_instances_stop_on_their_own_residual(cluster, coop):
     assert abs(tot1 - tot0) <= 1e-4 * tot0
 
 
-def test_no_handoff_with_a_fallback_budget():
+def test_no_handoff_while_a_fallback_restart_can_happen():
     descs = _descs(24, 3)
     h = eb.Handle.packing(descs, schedule=eb.SCHEDULE_INSTANCE)
     h.set_tail_handoff(8)
-    h.set_fallback(5000)
+    h.set_fallback(5000)  # a budget beyond the call's sweeps: no restart can happen, the hand-off runs
+    h.solve(300, -1.0)
+    assert h.tail_handoffs() >= 1
+    assert all(s["iterations"] == 300 for s in h.instance_stats())
+    h.set_fallback(100)  # restarts inside the launch: the per-instance schedule keeps every instance
     h.solve(300, -1.0)
     assert h.tail_handoffs() == 0
     assert all(s["iterations"] == 300 for s in h.instance_stats())
