@@ -311,10 +311,13 @@ def run_ttr(local: int, world: int = 1, rank: int = 0):
     # distribution (probe = full solves to the tolerance; untimed, like
     # creating the handle), used by both arms
     tune_all = learned.make_instances(TTR_INSTANCES, TTR_SEED + 1)
+    # tail hand-off: the last 1/16 of the instances still running finish
+    # together on the grid-wide schedule (paradmm_gpu_set_tail_handoff)
+    handoff = max(1, len(inst) // 16)
     tune = learned.tune([tune_all[i] for i in split_instances([d["n_circles"] for d in tune_all], world, rank)],
-                        TTR_MAXITER, TTR_TOL, device=local)
+                        TTR_MAXITER, TTR_TOL, device=local, handoff=handoff)
     kw = dict(schedule=tune["schedule"], cluster=tune["cluster_size"], coop_min_n=tune["coop_min_n"],
-              block_width=tune["block_width"])
+              block_width=tune["block_width"], handoff=handoff)
     net = learned.SetMLP(device=local)
     net.load()
     for _ in range(2):
@@ -345,7 +348,8 @@ def run_ttr(local: int, world: int = 1, rank: int = 0):
             "schedule": {"schedule": {1: "grid", 2: "instance", 3: "onchip"}.get(tune["schedule"], str(tune["schedule"])),
                          "block_width": tune["block_width"],
                          "cluster": tune["cluster_size"],
-                         "coop_min_n": tune["coop_min_n"], "autotune_candidates": tune["candidates"],
+                         "coop_min_n": tune["coop_min_n"], "tail_handoff": handoff,
+                         "autotune_candidates": tune["candidates"],
                          "probe_ms_best": tune["ms"], "probe_ms_worst": tune["worst_ms"]},
             "plain_s": plain_s, "learned_s": learned_s, "speedup": plain_s / learned_s,
             "converged_plain": int(sum(x[1] for x in P)), "converged_learned": int(sum(x[1] for x in L)),

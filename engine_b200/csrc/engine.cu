@@ -833,6 +833,7 @@ extern "C" int paradmm_gpu_create_packing(const paradmm_packing_desc *descs, int
     for (int i = 0; i < count; ++i) pk_add_desc(P, descs[i], i);
     rc = pk_finalize_build(h);
     P.use_graphs = h->opts.reserved[1] ? 0 : 1;
+    P.tail_yield = std::max(0, h->opts.reserved[2]);
     if (rc == PARADMM_OK) rc = pk_init_all(h, 0);
     if (rc) { free_handle_memory(h); delete h->pk; delete h; return rc; }
     h->num_dims = 2;

@@ -97,7 +97,8 @@ def _descs(instances):
 class Batch:
     """A packing handle over a list of instances (plain start)."""
 
-    def __init__(self, instances, device=0, schedule=0, cluster=0, coop_min_n=0, no_graphs=False, block_width=0):
+    def __init__(self, instances, device=0, schedule=0, cluster=0, coop_min_n=0, no_graphs=False, block_width=0,
+                 handoff=0):
         from . import opts
         self.lib = load()
         self.instances = instances
@@ -105,6 +106,7 @@ class Batch:
         o = opts(device=device, schedule=schedule, cluster_size=cluster, block_width=block_width)
         o.reserved[0] = coop_min_n
         o.reserved[1] = 1 if no_graphs else 0
+        o.reserved[2] = int(handoff)  # tail hand-off (paradmm_gpu_set_tail_handoff)
         p = C.c_void_p()
         check(self.lib.paradmm_gpu_create_packing(arr, len(instances), C.byref(o), C.byref(p)))
         self.h = p
@@ -350,13 +352,15 @@ def train_weights(n_instances: int = 20000, epochs: int = 40, seed: int = 100000
                 candidates=report, out=out)
 
 
-def tune(instances, sweeps: int, tol: float, device: int = 0) -> dict:
+def tune(instances, sweeps: int, tol: float, device: int = 0, handoff: int = 0) -> dict:
     """Tile side and schedule for batches like `instances`
-    (paradmm_gpu_create_packing_tuned with probe solve(sweeps, tol))."""
+    (paradmm_gpu_create_packing_tuned with probe solve(sweeps, tol)); the
+    probes of the per-instance schedule run with the tail hand-off `handoff`."""
     from . import Tuning, opts
     lib = load()
     arr, keep = _descs(instances)
     o = opts(device=device)
+    o.reserved[2] = int(handoff)
     p = C.c_void_p()
     t = Tuning()
     check(lib.paradmm_gpu_create_packing_tuned(arr, len(instances), C.byref(o), int(sweeps), float(tol), C.byref(p),

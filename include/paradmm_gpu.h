@@ -77,7 +77,8 @@ typedef struct paradmm_gpu_opts {
     int schedule;     /* packing engine: PARADMM_SCHEDULE_*                      */
     int cluster_size; /* per-instance schedule: CTAs per large instance (1, 2, 4, 8); 0 = default (2) */
     int reserved[6];  /* reserved[0]: per-instance schedule, smallest N solved by a whole cluster (0 = 200);
-                         reserved[1]: 1 = launch per-instance solves directly, not as a replayed CUDA graph */
+                         reserved[1]: 1 = launch per-instance solves directly, not as a replayed CUDA graph;
+                         reserved[2]: tail hand-off of the per-instance schedule (paradmm_gpu_set_tail_handoff) */
 } paradmm_gpu_opts;
 
 /* How the packing engine spreads a handle's instances over the GPU. */
