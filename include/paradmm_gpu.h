@@ -325,8 +325,10 @@ int64_t paradmm_gpu_launches(const paradmm_gpu *h);
  * pass over all their tiles by every CTA per sweep, instead of one pass per
  * instance by its own few CTAs); each keeps its own budget of maxiter sweeps
  * and its own stop test.  0 (default): off.  Not combined with a fallback
- * budget (paradmm_gpu_set_fallback).  paradmm_gpu_tail_handoffs: instances
- * the last solve call handed over. */
+ * budget (paradmm_gpu_set_fallback) that can restart an instance within the
+ * call.  The per-instance device timestamps (paradmm_gpu_instance_times)
+ * of a handed-over instance end at the hand-off.  paradmm_gpu_tail_handoffs:
+ * instances the last solve call handed over. */
 int paradmm_gpu_set_tail_handoff(paradmm_gpu *h, int instances);
 int paradmm_gpu_tail_handoffs(const paradmm_gpu *h);
 
