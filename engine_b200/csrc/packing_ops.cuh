@@ -56,10 +56,19 @@ PDM_D void wall_prox(float nx, float ny, float nr, float4 vp, float rc, float rr
 
 // max_alpha_radius (packing/host.c:10-29): ten Newton steps on the prox of
 // -r^a; r^(a-1) and r^(a-2) are exact for a = 2 (r, 1) and a = 1 (1, 1/r).
+// For a = 2 the Newton function -r + (rho/a)(r - n) is linear in r, so the
+// first step lands on its root rho n / (rho - 2) and the other nine move r by
+// rounding only: one step is taken (ten FP32 divisions were two thirds of a
+// small instance's consensus).  a = 1 keeps the ten steps, which carry the
+// reference's NaN at n = 0 (1/r at r = 0).
 PDM_D float radius_prox(float n, float rho, float a)
 {
     float r = fabsf(n * 0.5f);
     const float ra = rho / a;
+    if (a == 2.0f) {
+        r -= (-r + ra * (r - n)) / (-1.0f + ra);
+        return r < 0.0f ? 0.0f : r;
+    }
     for (int it = 0; it < 10; ++it) {
         float p1, p2;
         if (a == 2.0f) { p1 = r; p2 = 1.0f; }
