@@ -1258,7 +1258,7 @@ static int pk_run_grid(paradmm_gpu *h, long long n, double tol, int check_every,
         R.bal_mu = P.bal_mu;
         R.bal_lmin = P.bal_lmin;
         R.bal_lmax = P.bal_lmax;
-    R.bal_any = pk_bal_any(P);
+        R.bal_any = pk_bal_any(P);
         PDM_CUDA(cudaEventRecord(h->ev0, h->stream));
         cudaError_t e = pk_launch_persistent(P.V, P.stream_hint, Dv ? *Dv : P.D, R, P.grid, h->stream);
         if (e != cudaSuccess) return pdm_cuda_fail(e, "packing persistent launch", __FILE__, __LINE__);
