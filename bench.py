@@ -286,6 +286,7 @@ def run_reference_arm(args):
 # plain start only lengthened the batch (0.43 s with a 3000-sweep budget, 0.36 s
 # without, device time)
 TTR_INSTANCES, TTR_SEED, TTR_MAXITER, TTR_TOL, TTR_BUDGET = 512, 900000, 20000, 1e-5, 0
+TTR_REPS = 3  # timed rounds of each arm (after one untimed round); the median is reported
 
 
 def run_ttr(local: int, world: int = 1, rank: int = 0):
@@ -320,14 +321,20 @@ def run_ttr(local: int, world: int = 1, rank: int = 0):
               block_width=tune["block_width"], handoff=handoff)
     net = learned.SetMLP(device=local)
     net.load()
-    for _ in range(2):
+    # one untimed round, then TTR_REPS timed rounds of both arms, interleaved;
+    # each arm's figure is the median round (host wall clock, max over ranks)
+    walls_p, walls_l = [], []
+    for rep in range(1 + TTR_REPS):
         barrier(world)
         pl = learned.solve_plain(inst, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local, **kw)
         barrier(world)
         le = learned.solve_learned(inst, net, budget=TTR_BUDGET, maxiter=TTR_MAXITER, tol=TTR_TOL, device=local, **kw)
+        if rep > 0:
+            walls_p.append(allreduce_max(world, pl["wall_s"]))
+            walls_l.append(allreduce_max(world, le["wall_s"]))
     net.close()
-    plain_s = allreduce_max(world, pl["wall_s"])
-    learned_s = allreduce_max(world, le["wall_s"])
+    plain_s = statistics.median(walls_p)
+    learned_s = statistics.median(walls_l)
 
     def rows(res):
         return [(s["iterations"], int(s["converged"]), float(s["max_violation"]), float(c[:, 2].sum()),
@@ -351,7 +358,9 @@ def run_ttr(local: int, world: int = 1, rank: int = 0):
                          "coop_min_n": tune["coop_min_n"], "tail_handoff": handoff,
                          "autotune_candidates": tune["candidates"],
                          "probe_ms_best": tune["ms"], "probe_ms_worst": tune["worst_ms"]},
-            "plain_s": plain_s, "learned_s": learned_s, "speedup": plain_s / learned_s,
+            "plain_s": plain_s,
+            "plain_s_rounds": walls_p,
+            "learned_s_rounds": walls_l, "learned_s": learned_s, "speedup": plain_s / learned_s,
             "converged_plain": int(sum(x[1] for x in P)), "converged_learned": int(sum(x[1] for x in L)),
             "fallbacks": int(sum(x[4] for x in L)),
             "median_sweeps_plain": int(np.median(its_p)), "median_sweeps_learned": int(np.median(its_l)),
