@@ -206,3 +206,21 @@ def test_packing_desc_validation():
     d = (eb.PackingDesc * 1)()
     d[0].n_circles = 1
     assert lib.paradmm_gpu_create_packing(d, 1, None, C.byref(h)) == eb.EINVAL
+
+
+def test_fused_shard_and_tail_handoff_arguments_are_checked_without_a_device():
+    """The fused shard run, its buffers, the IPC helpers and the tail
+    hand-off validate their arguments before any device work."""
+    lib = eb.load()
+    vp = C.c_void_p
+    assert lib.paradmm_gpu_shard_run_fused(None, 1, None, None, 0, None) == eb.EINVAL
+    hs = (vp * 1)()
+    assert lib.paradmm_gpu_shard_run_fused(hs, 0, None, None, 0, None) == eb.EINVAL  # nlocal < 1
+    assert lib.paradmm_gpu_shard_run_fused(hs, 9, None, None, 0, None) == eb.EINVAL  # more than 8 ranks
+    assert lib.paradmm_gpu_shard_run_fused(hs, 1, None, None, 0, None) == eb.EINVAL  # no buffers
+    ex, fl = vp(), vp()
+    assert lib.paradmm_gpu_shard_fused_buffers(None, C.byref(ex), C.byref(fl)) == eb.EINVAL
+    assert lib.paradmm_gpu_ipc_export(None, C.create_string_buffer(64)) == eb.EINVAL
+    assert lib.paradmm_gpu_ipc_import(0, None, C.byref(ex)) == eb.EINVAL
+    assert lib.paradmm_gpu_set_tail_handoff(None, 8) == eb.EINVAL
+    assert lib.paradmm_gpu_tail_handoffs(None) == 0
