@@ -121,7 +121,9 @@ class Clocks:
         self.run = True
         self.t = threading.Thread(target=self._poll, daemon=True)
         self.t.start()
-        time.sleep(0.01)
+        t_wait = time.perf_counter()
+        while self.run and len(self.rows) < 3 and time.perf_counter() - t_wait < 2.0:  # sampling under way
+            time.sleep(0.001)
 
     def _poll(self):
         nv = self.nv
@@ -145,6 +147,9 @@ class Clocks:
     def stop(self, t0: float, t1: float) -> dict:
         if not self.run and not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "no samples"], "samples": 0}
+        t_wait = time.perf_counter()  # a sample after the region, when the poller is still running
+        while self.run and not any(r[0] > t1 for r in self.rows[-4:]) and time.perf_counter() - t_wait < 1.0:
+            time.sleep(0.001)
         self.run = False
         self.t.join(timeout=5)
         try:
