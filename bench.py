@@ -63,7 +63,7 @@ REF_BUDGET_S = 150.0    # reference arm: cap on the timed sweeps' CPU time
 # launch of NCU_SWEEPS sweeps of this workload (N = 8000, bench seed), from one
 # ncu capture of `bench.py --steps 20 --warmup 3 --no-e2e --no-ttr --no-cpu`;
 # profiles/pk_persistent_n8000_dram.md has the command and the figures.
-NCU_DRAM_BYTES_N8000 = 15_401_815_040 + 15_766_901_504
+NCU_DRAM_BYTES_N8000 = 15_403_251_456 + 15_773_677_824
 NCU_SWEEPS = 20
 
 
