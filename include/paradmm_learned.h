@@ -8,7 +8,7 @@
  * own position and radius, nearest-neighbour and wall distances, a
  * neighbour-repulsion vector, density counts, N and box aspect) to a guess of
  * the packing plain ADMM converges to.  The guess warm-starts the engine
- * (paradmm_gpu_warm_start); the ADMM residual judges it, and instances that
+ * (paradmm_gpu_warm_start); the ADMM residual decides, and instances that
  * do not converge within their budget are re-solved from the plain start.
  * Training (forward, backward, Adam) runs on the GPU with this library's own
  * kernels on packings the plain solver produced.
